@@ -1,0 +1,175 @@
+/*
+ * kifmm_b200 — C ABI of a B200 (sm_100a) evaluator for the kernel-independent
+ * fast multipole method, 3-D Laplace kernel phi(t) = sum_s w_s / (4 pi |t-s|).
+ *
+ * It replaces the GPU evaluator plug-in of the reference benchmark (the
+ * functions fmm/evaluate.h:18-57 declares and fmm/evaluate--cuda.cu,
+ * fmm/run--cuda.cu and fmm/cuda.cu implement for `fmmd--cuda`).  Those are C++
+ * symbols over std::vector trees; this ABI carries the same information as
+ * plain pointers and sizes.  Every call returns a status; nothing exits the
+ * process.  Host arrays belong to the caller, device memory belongs to the
+ * plan.  Calls on one plan are not re-entrant.  `stream` is a cudaStream_t
+ * passed as void* (NULL = legacy default stream).
+ */
+#ifndef KIFMM_B200_H
+#define KIFMM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  KFMM_OK = 0,
+  KFMM_ERR_INVALID = 1,     /* bad argument or inconsistent tree */
+  KFMM_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  KFMM_ERR_ALLOC = 3,       /* host or device allocation failed */
+  KFMM_ERR_UNSUPPORTED = 4, /* e.g. NP outside 3..8 */
+  KFMM_ERR_STATE = 5        /* call out of order (e.g. run before points) */
+} kfmm_status;
+
+typedef enum {
+  KFMM_PLAIN_FP64 = 0, /* FP64 throughout */
+  KFMM_MIXED = 1       /* FP32 + compensated sums for P2P and M2L products */
+} kfmm_precision;
+
+/* Point sets.  Generators restate fmm/input.cc:30-84 (create) and the density
+ * draw of fmm/driver.cc:244,266: srand48(seed) then the reference's drand48
+ * sequence.  distribution: "uniform" ([-1,1)^3), "ellipseUniformAngles",
+ * or "ellipsoidSurface" (semi-axes 0.5,0.5,0.05 centred at 0.5, densities in
+ * [-1,1); not in the reference).  coincide != 0 makes targets the sources
+ * (env C of fmm/util.c:177).  If check_ids is not NULL, num_check validation
+ * indices are drawn next from the same stream (fmm/driver.cc:149-152). */
+kfmm_status kfmm_generate_points(int n, const char* distribution, int coincide, long seed,
+                                 double* sx, double* sy, double* sz, double* den,
+                                 double* tx, double* ty, double* tz,
+                                 int num_check, int* check_ids);
+
+/* Octree + U/V/W/X lists: restates src_tree / trg_tree / compute_lists
+ * (fmm/input.cc:204-298, 304-381, 387-460).  Node order, point order, tags
+ * and lists are identical to the reference's vector<NodeTree>. */
+typedef struct kfmm_tree kfmm_tree;
+
+typedef struct {
+  int num_nodes;
+  int num_levels;      /* node_level has num_levels+1 entries */
+  int num_src, num_trg;
+  const int* parent;   /* -1 for the root */
+  const int* child;    /* first of 8 contiguous children, -1 for a leaf */
+  const int* depth;
+  const int* tag;      /* bit 1: has sources, bit 2: has targets */
+  const int* path;     /* 3 per node: path2Node */
+  const int* src_beg;  /* leaf-order source range (leaves only) */
+  const int* src_num;
+  const int* trg_beg;
+  const int* trg_num;
+  const int* src_perm; /* leaf-order position -> original source index */
+  const int* trg_perm; /* leaf-order position -> original target index */
+  const int* node_level;
+  const int *u_ptr, *u_idx; /* CSR lists, num_nodes+1 pointers each */
+  const int *v_ptr, *v_idx;
+  const int *w_ptr, *w_idx;
+  const int *x_ptr, *x_idx;
+} kfmm_tree_desc;
+
+kfmm_status kfmm_tree_build(int num_src, const double* sx, const double* sy,
+                            const double* sz, int num_trg, const double* tx,
+                            const double* ty, const double* tz, int pts_max,
+                            kfmm_tree** out);
+kfmm_status kfmm_tree_describe(const kfmm_tree* tree, kfmm_tree_desc* desc);
+void kfmm_tree_destroy(kfmm_tree* tree);
+
+/* Surface sizes for NP (fmm/trans.cc:26,67): P=|UE|=|DE|=|DC|, Q=|UC|,
+ * F = complex spectrum length (np+1)(2np)^2. */
+kfmm_status kfmm_sizes(int np, int* P, int* Q, int* F);
+
+/* FP64 host precompute of the translation operators (fmm/trans.cc:144-268,
+ * fmm/vecmatop.cc:34-78, fmm/omp_sse_block.cc:432-478).  Column-major like the
+ * reference: uc2ue P x Q, ue2uc 8 x (Q x P), dc2de P x P, de2dc 8 x (P x P),
+ * ue2dc 343 x F complex (interleaved re,im; zero where |delta|_inf <= 1).
+ * Any output pointer may be NULL. */
+kfmm_status kfmm_operators(int np, double* uc2ue, double* ue2uc, double* dc2de,
+                           double* de2dc, double* ue2dc);
+
+/* Plan = preproc (fmm/evaluate--cuda.cu:1441-2239): uploads tree, lists and
+ * operators to the current CUDA device and allocates every work array. */
+typedef struct kfmm_plan kfmm_plan;
+
+kfmm_status kfmm_plan_create(const kfmm_tree_desc* tree, int np, kfmm_precision precision,
+                             kfmm_plan** out);
+kfmm_status kfmm_plan_destroy(kfmm_plan* plan);
+
+/* Points in ORIGINAL order.  Host variants copy host->device inside the call
+ * (on `stream`); device variants take device pointers.  Targets are needed
+ * once per tree; densities may change between runs. */
+kfmm_status kfmm_set_sources(kfmm_plan* plan, const double* sx, const double* sy,
+                             const double* sz, const double* den, void* stream);
+kfmm_status kfmm_set_targets(kfmm_plan* plan, const double* tx, const double* ty,
+                             const double* tz, void* stream);
+kfmm_status kfmm_set_sources_device(kfmm_plan* plan, const double* sx, const double* sy,
+                                    const double* sz, const double* den, void* stream);
+kfmm_status kfmm_set_targets_device(kfmm_plan* plan, const double* tx, const double* ty,
+                                    const double* tz, void* stream);
+
+/* run (fmm/run--cuda.cu:27-345): every phase below, in order, asynchronously
+ * on `stream`; potentials stay on the device in original order. */
+kfmm_status kfmm_run(kfmm_plan* plan, void* stream);
+
+/* The phases, one by one (fmm/evaluate.h:35-52).  Call in this order. */
+kfmm_status kfmm_up_calc(kfmm_plan* plan, void* stream);    /* S2M + M2M */
+kfmm_status kfmm_vlist_calc(kfmm_plan* plan, void* stream); /* FFT, Hadamard, IFFT */
+kfmm_status kfmm_xlist_calc(kfmm_plan* plan, void* stream); /* S2L part of X */
+kfmm_status kfmm_down_calc(kfmm_plan* plan, void* stream);  /* L2L */
+/* U list + W list + direct part of X + L2T, fused: each target's potential is
+ * accumulated once, in registers, and written once. */
+kfmm_status kfmm_ulist_calc(kfmm_plan* plan, void* stream);
+/* copy_trg_val (fmm/cuda.cu:2543-2565): potentials to original order on the
+ * device; pot_host (may be NULL) additionally receives them (synchronous). */
+kfmm_status kfmm_copy_trg_val(kfmm_plan* plan, double* pot_host, void* stream);
+kfmm_status kfmm_get_potentials_device(kfmm_plan* plan, double* pot_dev, void* stream);
+
+/* End-to-end: host inputs (original order) -> host potentials. */
+kfmm_status kfmm_evaluate(kfmm_plan* plan, const double* sx, const double* sy,
+                          const double* sz, const double* den, const double* tx,
+                          const double* ty, const double* tz, double* pot, void* stream);
+
+/* ulist__direct_evaluation (fmm/evaluate.h:27): pot[i] += sum_j den[j] /
+ * (4 pi |t_i - s_j|), skipping r == 0.  Device pointers, FP64. */
+kfmm_status kfmm_direct_evaluation(int nt, const double* tx, const double* ty,
+                                   const double* tz, double* pot, int ns,
+                                   const double* sx, const double* sy, const double* sz,
+                                   const double* den, void* stream);
+
+/* Introspection for parity tests: copy a per-node array (node-major, P or Q
+ * doubles per node) to host.  which: 0 src_upw_equ_den, 1 trg_dwn_chk_val,
+ * 2 trg_dwn_equ_den, 3 potentials in leaf order, 4 source spectra (2F per
+ * node).  Synchronous. */
+kfmm_status kfmm_read_array(kfmm_plan* plan, int which, double* host_out, size_t count);
+
+typedef struct {
+  double u_pairs;      /* target-source pairs of the near-field kernel */
+  double s2m_pairs;    /* pairs of the S2M check-potential kernel */
+  double s2l_pairs;    /* pairs of the X-list S2L kernel */
+  double v_pairs;      /* V-list (target, source) box pairs */
+  double hadamard_cmacs; /* complex multiply-adds the Hadamard kernel issues */
+  double gemm_flops;   /* 2*m*n*k over all level GEMMs */
+  double spectra_bytes; /* source + target spectra bytes, one pass each */
+  int num_nodes, P, Q, F;
+  int launches;        /* kernels one kfmm_run launches */
+} kfmm_stats;
+kfmm_status kfmm_plan_stats(const kfmm_plan* plan, kfmm_stats* stats);
+
+/* Per-phase device times of the last kfmm_run with timing enabled (ms):
+ * [up, vlist, xlist, down, ulist, copy].  enable != 0 records CUDA events. */
+kfmm_status kfmm_enable_timing(kfmm_plan* plan, int enable);
+kfmm_status kfmm_phase_times(const kfmm_plan* plan, float* ms6);
+
+const char* kfmm_last_error(void);
+const char* kfmm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

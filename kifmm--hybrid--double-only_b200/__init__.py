@@ -1,0 +1,238 @@
+"""ctypes binding of libkifmm_b200.so (include/kifmm_b200.h).
+
+Python here is plumbing for tests and benchmarks: every computation runs in
+the C++/CUDA library.  Loading fails loudly if the library has not been built;
+there is no fallback path.
+
+The directory name is not a Python identifier, so importers load this file by
+path (see ``load_package`` in __graft_entry__.py) under the name
+``kifmm_b200``.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkifmm_b200.so")
+CLI_PATH = os.path.join(HERE, "fmmd--b200")
+
+PLAIN_FP64 = 0
+MIXED = 1
+
+_lib = None
+
+_i32p = ctypes.POINTER(ctypes.c_int)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+class KfmmError(RuntimeError):
+    pass
+
+
+class TreeDesc(ctypes.Structure):
+    _fields_ = [("num_nodes", ctypes.c_int), ("num_levels", ctypes.c_int),
+                ("num_src", ctypes.c_int), ("num_trg", ctypes.c_int)] + [
+        (n, _i32p) for n in ("parent", "child", "depth", "tag", "path", "src_beg", "src_num",
+                             "trg_beg", "trg_num", "src_perm", "trg_perm", "node_level",
+                             "u_ptr", "u_idx", "v_ptr", "v_idx", "w_ptr", "w_idx", "x_ptr",
+                             "x_idx")]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("u_pairs", "s2m_pairs", "s2l_pairs", "v_pairs",
+                                                "hadamard_cmacs", "gemm_flops",
+                                                "spectra_bytes")] + [
+        (n, ctypes.c_int) for n in ("num_nodes", "P", "Q", "F", "launches")]
+
+
+def lib():
+    """Load libkifmm_b200.so once; raise if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise KfmmError(f"{LIB_PATH} is not built; run kifmm--hybrid--double-only_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    sig = {
+        "kfmm_generate_points": [i, ctypes.c_char_p, i, ctypes.c_long] + [_f64p] * 7 + [i, _i32p],
+        "kfmm_tree_build": [i, _f64p, _f64p, _f64p, i, _f64p, _f64p, _f64p, i,
+                            ctypes.POINTER(vp)],
+        "kfmm_tree_describe": [vp, ctypes.POINTER(TreeDesc)],
+        "kfmm_sizes": [i, _i32p, _i32p, _i32p],
+        "kfmm_operators": [i, _f64p, _f64p, _f64p, _f64p, _f64p],
+        "kfmm_plan_create": [ctypes.POINTER(TreeDesc), i, i, ctypes.POINTER(vp)],
+        "kfmm_plan_destroy": [vp],
+        "kfmm_set_sources": [vp, _f64p, _f64p, _f64p, _f64p, vp],
+        "kfmm_set_targets": [vp, _f64p, _f64p, _f64p, vp],
+        "kfmm_set_sources_device": [vp, vp, vp, vp, vp, vp],
+        "kfmm_set_targets_device": [vp, vp, vp, vp, vp],
+        "kfmm_run": [vp, vp],
+        "kfmm_up_calc": [vp, vp],
+        "kfmm_vlist_calc": [vp, vp],
+        "kfmm_xlist_calc": [vp, vp],
+        "kfmm_down_calc": [vp, vp],
+        "kfmm_ulist_calc": [vp, vp],
+        "kfmm_copy_trg_val": [vp, _f64p, vp],
+        "kfmm_get_potentials_device": [vp, vp, vp],
+        "kfmm_evaluate": [vp] + [_f64p] * 8 + [vp],
+        "kfmm_direct_evaluation": [i, vp, vp, vp, vp, i, vp, vp, vp, vp, vp],
+        "kfmm_read_array": [vp, i, _f64p, ctypes.c_size_t],
+        "kfmm_plan_stats": [vp, ctypes.POINTER(Stats)],
+        "kfmm_enable_timing": [vp, i],
+        "kfmm_phase_times": [vp, ctypes.POINTER(ctypes.c_float)],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    L.kfmm_tree_destroy.argtypes = [vp]
+    L.kfmm_tree_destroy.restype = None
+    L.kfmm_last_error.restype = ctypes.c_char_p
+    L.kfmm_version.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def check(status, what=""):
+    if status != 0:
+        msg = lib().kfmm_last_error().decode()
+        raise KfmmError(f"{what}: status {status}: {msg}")
+
+
+def _p(a, t=_f64p):
+    return a.ctypes.data_as(t)
+
+
+def sizes(np_):
+    P, Q, F = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    check(lib().kfmm_sizes(np_, ctypes.byref(P), ctypes.byref(Q), ctypes.byref(F)), "sizes")
+    return P.value, Q.value, F.value
+
+
+def generate_points(n, distribution="uniform", coincide=0, seed=26, num_check=0):
+    """Reference generators (drand48 stream): dict of float64 arrays."""
+    out = {k: np.empty(n, np.float64) for k in ("sx", "sy", "sz", "den", "tx", "ty", "tz")}
+    ids = np.empty(max(num_check, 1), np.int32)
+    check(lib().kfmm_generate_points(n, distribution.encode(), coincide, seed,
+                                     *[_p(out[k]) for k in ("sx", "sy", "sz", "den", "tx", "ty",
+                                                            "tz")],
+                                     num_check, _p(ids, _i32p)), "generate_points")
+    out["check_ids"] = ids[:num_check]
+    return out
+
+
+def operators(np_):
+    P, Q, F = sizes(np_)
+    o = {"uc2ue": np.empty(P * Q), "ue2uc": np.empty(8 * Q * P), "dc2de": np.empty(P * P),
+         "de2dc": np.empty(8 * P * P), "ue2dc": np.empty(343 * 2 * F)}
+    check(lib().kfmm_operators(np_, *[_p(o[k]) for k in ("uc2ue", "ue2uc", "dc2de", "de2dc",
+                                                         "ue2dc")]), "operators")
+    return o
+
+
+class Tree:
+    """Octree + interaction lists built by the library (fmm/input.cc)."""
+
+    def __init__(self, sx, sy, sz, tx, ty, tz, pts_max):
+        self._arrays = [np.ascontiguousarray(a, np.float64) for a in (sx, sy, sz, tx, ty, tz)]
+        sx, sy, sz, tx, ty, tz = self._arrays
+        h = ctypes.c_void_p()
+        check(lib().kfmm_tree_build(len(sx), _p(sx), _p(sy), _p(sz), len(tx), _p(tx), _p(ty),
+                                    _p(tz), pts_max, ctypes.byref(h)), "tree_build")
+        self.handle = h
+        self.desc = TreeDesc()
+        check(lib().kfmm_tree_describe(h, ctypes.byref(self.desc)), "tree_describe")
+
+    def array(self, name):
+        d = self.desc
+        nn = d.num_nodes
+        n = {"path": 3 * nn, "src_perm": d.num_src, "trg_perm": d.num_trg,
+             "node_level": d.num_levels + 1}.get(name, nn)
+        if name.endswith("_ptr"):
+            n = nn + 1
+        if name.endswith("_idx"):
+            n = self.array(name[:-4] + "_ptr")[-1]
+        ptr = getattr(d, name)
+        return np.ctypeslib.as_array(ptr, shape=(int(n),)).copy() if n > 0 else np.zeros(0, np.int32)
+
+    def close(self):
+        if self.handle:
+            lib().kfmm_tree_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan:
+    """An evaluation plan on the current CUDA device."""
+
+    def __init__(self, tree, np_, precision=PLAIN_FP64):
+        self.tree = tree
+        self.np = np_
+        h = ctypes.c_void_p()
+        check(lib().kfmm_plan_create(ctypes.byref(tree.desc), np_, precision, ctypes.byref(h)),
+              "plan_create")
+        self.handle = h
+        self.nt = tree.desc.num_trg
+        self.ns = tree.desc.num_src
+
+    def set_points(self, pts, stream=None):
+        a = {k: np.ascontiguousarray(pts[k], np.float64) for k in ("sx", "sy", "sz", "den", "tx",
+                                                                    "ty", "tz")}
+        self._hold = a
+        check(lib().kfmm_set_targets(self.handle, _p(a["tx"]), _p(a["ty"]), _p(a["tz"]), stream),
+              "set_targets")
+        check(lib().kfmm_set_sources(self.handle, _p(a["sx"]), _p(a["sy"]), _p(a["sz"]),
+                                     _p(a["den"]), stream), "set_sources")
+
+    def run(self, stream=None):
+        check(lib().kfmm_run(self.handle, stream), "run")
+
+    def potentials(self, stream=None):
+        out = np.empty(self.nt, np.float64)
+        check(lib().kfmm_copy_trg_val(self.handle, _p(out), stream), "copy_trg_val")
+        return out
+
+    def evaluate(self, pts, stream=None):
+        a = {k: np.ascontiguousarray(pts[k], np.float64) for k in ("sx", "sy", "sz", "den", "tx",
+                                                                    "ty", "tz")}
+        out = np.empty(self.nt, np.float64)
+        check(lib().kfmm_evaluate(self.handle, *[_p(a[k]) for k in ("sx", "sy", "sz", "den",
+                                                                     "tx", "ty", "tz")],
+                                  _p(out), stream), "evaluate")
+        return out
+
+    def read(self, which, count):
+        out = np.empty(count, np.float64)
+        check(lib().kfmm_read_array(self.handle, which, _p(out), count), "read_array")
+        return out
+
+    def stats(self):
+        s = Stats()
+        check(lib().kfmm_plan_stats(self.handle, ctypes.byref(s)), "plan_stats")
+        return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def enable_timing(self, on=True):
+        check(lib().kfmm_enable_timing(self.handle, 1 if on else 0), "enable_timing")
+
+    def phase_times(self):
+        ms = (ctypes.c_float * 6)()
+        check(lib().kfmm_phase_times(self.handle, ms), "phase_times")
+        return dict(zip(("up", "vlist", "xlist", "down", "ulist", "copy"), list(ms)))
+
+    def close(self):
+        if self.handle:
+            lib().kfmm_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

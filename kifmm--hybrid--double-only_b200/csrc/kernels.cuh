@@ -1,0 +1,477 @@
+// Device kernels of the KIFMM evaluator (sm_100a).  Included by plan.cu only.
+//
+// Data layout in HBM (all node-major, node = index into the BFS node array):
+//   src4[i]      leaf-ordered sources (x, y, z, w)            double4
+//   trg4[i]      leaf-ordered targets (x, y, z, 0)            double4
+//   ctr[n]       node centre and radius (cx, cy, cz, r)       double4
+//   uden/dchk/dden[n*P + k]   upward equivalent density, downward check
+//                potential, downward equivalent density      double
+//   spec/effv[n*F + f]        source / target spectra         double2
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace kfmm {
+
+constexpr double kOOFP = 1.0 / (4.0 * 3.14159265358979323846);
+
+// ---------------------------------------------------------------------------
+// P2P engine.  A job evaluates one set of targets against a list of source
+// sets ("entries").  Targets: real points of a leaf (kind 0) or the UC (1) /
+// DC (2) check surface of a node.  Entries: (kind << 28) | node, kind 0 =
+// the node's source points, 1 = the node's UE surface carrying uden, 2 = the
+// node's DE surface carrying dden.  Output: out[job.out + i] = (or +=)
+// 1/(4 pi) sum_j w_j / |t_i - s_j|, pairs with r == 0 skipped
+// (fmm/omp.cc:259-283).
+// ---------------------------------------------------------------------------
+struct P2PJob {
+  int tnode, tkind, tbeg, tcnt;
+  int ebeg, eend, out, mode;  // mode 0 write, 1 add
+};
+
+struct P2PParams {
+  const P2PJob* jobs;
+  const int* entries;
+  const double4* src4;
+  const double4* trg4;
+  const double4* ctr;
+  const int* src_beg;
+  const int* src_num;
+  const double* uden;
+  const double* dden;
+  const double* sp_ue;  // 3 per point
+  const double* sp_uc;
+  const double* sp_de;
+  const double* sp_dc;
+  double* out;
+  int P, Q;
+};
+
+constexpr int kP2PThreads = 128;
+constexpr int kP2PStage = 512;
+
+__device__ __forceinline__ double3 surface_point(const double4 c, const double* sp, int k) {
+  // centre + radius * unit-surface point, unfused as fmm/trans.cc:92-100
+  double3 r;
+  r.x = __dadd_rn(c.x, __dmul_rn(c.w, sp[3 * k]));
+  r.y = __dadd_rn(c.y, __dmul_rn(c.w, sp[3 * k + 1]));
+  r.z = __dadd_rn(c.z, __dmul_rn(c.w, sp[3 * k + 2]));
+  return r;
+}
+
+__global__ void __launch_bounds__(kP2PThreads)
+p2p_fp64_kernel(P2PParams p) {
+  __shared__ double4 stage[kP2PStage];
+  const P2PJob J = p.jobs[blockIdx.x];
+  const int tid = threadIdx.x;
+  const bool active = tid < J.tcnt;
+  const bool warp_active = (tid & ~31) < J.tcnt;
+  double tx = 0, ty = 0, tz = 0;
+  if (active) {
+    if (J.tkind == 0) {
+      double4 t = p.trg4[J.tbeg + tid];
+      tx = t.x;
+      ty = t.y;
+      tz = t.z;
+    } else {
+      double3 s = surface_point(p.ctr[J.tnode], J.tkind == 1 ? p.sp_uc : p.sp_dc, J.tbeg + tid);
+      tx = s.x;
+      ty = s.y;
+      tz = s.z;
+    }
+  }
+  double acc = 0.0;
+  int fill = 0;
+  auto consume = [&](int m) {
+    __syncthreads();
+    if (warp_active) {
+#pragma unroll 4
+      for (int j = 0; j < m; ++j) {
+        const double4 s = stage[j];
+        const double dx = tx - s.x, dy = ty - s.y, dz = tz - s.z;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const double inv = rsqrt(r2);
+        acc = fma(s.w, r2 > 0.0 ? inv : 0.0, acc);
+      }
+    }
+    __syncthreads();
+  };
+  for (int e = J.ebeg; e < J.eend; ++e) {
+    const int ent = p.entries[e];
+    const int kind = ent >> 28, node = ent & 0x0fffffff;
+    int count, base = 0;
+    if (kind == 0) {
+      count = p.src_num[node];
+      base = p.src_beg[node];
+    } else {
+      count = p.P;
+    }
+    int done = 0;
+    while (done < count) {
+      const int m = min(count - done, kP2PStage - fill);
+      for (int k = tid; k < m; k += kP2PThreads) {
+        double4 v;
+        if (kind == 0) {
+          v = p.src4[base + done + k];
+        } else {
+          const double4 c = p.ctr[node];
+          const double3 s = surface_point(c, kind == 1 ? p.sp_ue : p.sp_de, done + k);
+          v.x = s.x;
+          v.y = s.y;
+          v.z = s.z;
+          v.w = (kind == 1 ? p.uden : p.dden)[(size_t)node * p.P + done + k];
+        }
+        stage[fill + k] = v;
+      }
+      fill += m;
+      done += m;
+      if (fill == kP2PStage) {
+        consume(fill);
+        fill = 0;
+      }
+    }
+  }
+  if (fill > 0) consume(fill);
+  if (active) {
+    const double r = kOOFP * acc;
+    double* o = p.out + J.out + tid;
+    if (J.mode) *o += r;
+    else *o = r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Level GEMM on FP64 tensor cores (mma.sync m8n8k4 DMMA):
+//   C[:, j] = alpha_j * A * B[:, j]   (+ C[:, j] when accumulate)
+// A: M x K column-major (lda = M).  Column j of B starts at B + boff[j]
+// (K contiguous values), column j of C at C + coff[j] (M values).
+// ---------------------------------------------------------------------------
+struct GemmArgs {
+  const double* A;
+  int M, K;
+  const double* B;
+  const int* boff;
+  double* C;
+  const int* coff;
+  const double* alpha;  // per column, or NULL -> alpha_const
+  double alpha_const;
+  int ncol;
+  int accumulate;
+};
+
+constexpr int kGemmBM = 64, kGemmBN = 32, kGemmBK = 16;
+
+__device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(128) gemm_fp64_dmma_kernel(GemmArgs g) {
+  __shared__ double As[kGemmBK][kGemmBM + 4];
+  __shared__ double Bs[kGemmBN][kGemmBK + 1];
+  __shared__ int boff_s[kGemmBN];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * kGemmBN;
+  if (tid < kGemmBN) boff_s[tid] = (n0 + tid < g.ncol) ? g.boff[n0 + tid] : -1;
+  double acc[4][2][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  __syncthreads();
+  for (int k0 = 0; k0 < g.K; k0 += kGemmBK) {
+#pragma unroll
+    for (int r = 0; r < (kGemmBK * kGemmBM) / 128; ++r) {
+      const int idx = tid + r * 128;
+      const int m = idx % kGemmBM, k = idx / kGemmBM;
+      const int gm = m0 + m, gk = k0 + k;
+      As[k][m] = (gm < g.M && gk < g.K) ? g.A[(size_t)gk * g.M + gm] : 0.0;
+    }
+#pragma unroll
+    for (int r = 0; r < (kGemmBK * kGemmBN) / 128; ++r) {
+      const int idx = tid + r * 128;
+      const int k = idx % kGemmBK, n = idx / kGemmBK;
+      const int gk = k0 + k;
+      const int bo = boff_s[n];
+      Bs[n][k] = (bo >= 0 && gk < g.K) ? g.B[(size_t)bo + gk] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kGemmBK; kk += 4) {
+      double af[4], bf[2];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) af[mi] = As[kk + (lane & 3)][wm * 32 + mi * 8 + (lane >> 2)];
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) bf[ni] = Bs[wn * 16 + ni * 8 + (lane >> 2)][kk + (lane & 3)];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni) dmma_884(acc[mi][ni][0], acc[mi][ni][1], af[mi], bf[ni]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int m = m0 + wm * 32 + mi * 8 + (lane >> 2);
+        const int n = n0 + wn * 16 + ni * 8 + (lane & 3) * 2 + h;
+        if (m < g.M && n < g.ncol) {
+          const double a = g.alpha ? g.alpha[n] : g.alpha_const;
+          double* c = g.C + (size_t)g.coff[n] + m;
+          const double v = a * acc[mi][ni][h];
+          if (g.accumulate) *c += v;
+          else *c = v;
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
+// V list.  Grids: the (2np)^3 regular grid, x fastest; surface sample (i,j,k)
+// sits at (x,y,z) = (i,j,k) + np/2 (fmm/trans.cc:336-358, 395-418).
+// Spectrum index (kz * n + ky) * (np + 1) + kx (r2c halves x).
+// Both transforms are pruned to the np^3 block that holds the surface.
+// ---------------------------------------------------------------------------
+struct FFTParams {
+  int np, P, F;
+  const int* nodes;   // nodes to transform
+  const int* depth;
+  const int* surf_idx;  // np^3 -> surface index or -1, index (i*np + j)*np + k
+  const int* surf_ijk;  // P x 3
+  const double* cs;     // cos(2 pi m / n), m < n
+  const double* sn;     // sin(2 pi m / n)
+  const double* pln;    // uden (forward) or dchk target (inverse) base
+  double* plnout;
+  const double2* specin;
+  double2* specout;
+};
+
+constexpr int kFFTThreads = 128;
+constexpr int kMaxNP = 8;
+
+// uden * 2^depth -> scatter -> r2c (omp.cc:386-428, trans.cc:309-358)
+__global__ void __launch_bounds__(kFFTThreads) fft_src_fp64_kernel(FFTParams p) {
+  __shared__ double den[kMaxNP * kMaxNP * kMaxNP];
+  __shared__ double2 X[kMaxNP * kMaxNP * (kMaxNP + 1)];
+  __shared__ double2 Y[kMaxNP * 2 * kMaxNP * (kMaxNP + 1)];
+  __shared__ double cs[2 * kMaxNP], sn[2 * kMaxNP];
+  const int np = p.np, n = 2 * np, h = np / 2, nk = np + 1;
+  const int node = p.nodes[blockIdx.x];
+  const double scale = ldexp(1.0, p.depth[node]);
+  const int tid = threadIdx.x;
+  if (tid < n) {
+    cs[tid] = p.cs[tid];
+    sn[tid] = p.sn[tid];
+  }
+  for (int q = tid; q < np * np * np; q += kFFTThreads) {
+    const int s = p.surf_idx[q];
+    den[q] = s >= 0 ? p.pln[(size_t)node * p.P + s] * scale : 0.0;
+  }
+  __syncthreads();
+  // x pass: (k=z, j=y) rows, kx outputs, sum over i=x
+  for (int q = tid; q < np * np * nk; q += kFFTThreads) {
+    const int kx = q % nk, j = (q / nk) % np, k = q / (nk * np);
+    double ar = 0, ai = 0;
+    for (int i = 0; i < np; ++i) {
+      const double v = den[(i * np + j) * np + k];
+      const int m = (kx * (i + h)) % n;
+      ar += v * cs[m];
+      ai -= v * sn[m];
+    }
+    X[(k * np + j) * nk + kx] = make_double2(ar, ai);
+  }
+  __syncthreads();
+  // y pass
+  for (int q = tid; q < np * n * nk; q += kFFTThreads) {
+    const int kx = q % nk, ky = (q / nk) % n, k = q / (nk * n);
+    double ar = 0, ai = 0;
+    for (int j = 0; j < np; ++j) {
+      const double2 v = X[(k * np + j) * nk + kx];
+      const int m = (ky * (j + h)) % n;
+      ar += v.x * cs[m] + v.y * sn[m];
+      ai += v.y * cs[m] - v.x * sn[m];
+    }
+    Y[(k * n + ky) * nk + kx] = make_double2(ar, ai);
+  }
+  __syncthreads();
+  // z pass -> spectrum
+  double2* out = p.specout + (size_t)node * p.F;
+  for (int q = tid; q < n * n * nk; q += kFFTThreads) {
+    const int kx = q % nk, ky = (q / nk) % n, kz = q / (nk * n);
+    double ar = 0, ai = 0;
+    for (int k = 0; k < np; ++k) {
+      const double2 v = Y[(k * n + ky) * nk + kx];
+      const int m = (kz * (k + h)) % n;
+      ar += v.x * cs[m] + v.y * sn[m];
+      ai += v.y * cs[m] - v.x * sn[m];
+    }
+    out[q] = make_double2(ar, ai);
+  }
+}
+
+// spectrum -> c2r -> gather at the DC surface, scaled by 1/(2np)^3
+// (omp.cc:482-533, trans.cc:383-418).  Writes plnout[node*P + s].
+__global__ void __launch_bounds__(kFFTThreads) ifft_trg_fp64_kernel(FFTParams p) {
+  extern __shared__ double2 dyn[];
+  __shared__ double2 W[kMaxNP * kMaxNP * (kMaxNP + 1)];
+  __shared__ double cs[2 * kMaxNP], sn[2 * kMaxNP];
+  const int np = p.np, n = 2 * np, h = np / 2, nk = np + 1;
+  const int node = p.nodes[blockIdx.x];
+  const int tid = threadIdx.x;
+  double2* E = dyn;                 // F
+  double2* Z = dyn + p.F;           // np * n * nk
+  if (tid < n) {
+    cs[tid] = p.cs[tid];
+    sn[tid] = p.sn[tid];
+  }
+  const double2* in = p.specin + (size_t)node * p.F;
+  for (int q = tid; q < p.F; q += kFFTThreads) E[q] = in[q];
+  __syncthreads();
+  // z inverse, only z in the surface block
+  for (int q = tid; q < np * n * nk; q += kFFTThreads) {
+    const int kx = q % nk, ky = (q / nk) % n, k = q / (nk * n);
+    double ar = 0, ai = 0;
+    for (int kz = 0; kz < n; ++kz) {
+      const double2 v = E[(kz * n + ky) * nk + kx];
+      const int m = (kz * (k + h)) % n;
+      ar += v.x * cs[m] - v.y * sn[m];
+      ai += v.y * cs[m] + v.x * sn[m];
+    }
+    Z[(k * n + ky) * nk + kx] = make_double2(ar, ai);
+  }
+  __syncthreads();
+  // y inverse
+  for (int q = tid; q < np * np * nk; q += kFFTThreads) {
+    const int kx = q % nk, j = (q / nk) % np, k = q / (nk * np);
+    double ar = 0, ai = 0;
+    for (int ky = 0; ky < n; ++ky) {
+      const double2 v = Z[(k * n + ky) * nk + kx];
+      const int m = (ky * (j + h)) % n;
+      ar += v.x * cs[m] - v.y * sn[m];
+      ai += v.y * cs[m] + v.x * sn[m];
+    }
+    W[(k * np + j) * nk + kx] = make_double2(ar, ai);
+  }
+  __syncthreads();
+  // x: Hermitian half -> real, at surface points only
+  const double inv_g = 1.0 / (double)(n * n * n);
+  for (int s = tid; s < p.P; s += kFFTThreads) {
+    const int i = p.surf_ijk[3 * s], j = p.surf_ijk[3 * s + 1], k = p.surf_ijk[3 * s + 2];
+    const double2* w = &W[(k * np + j) * nk];
+    const int x = i + h;
+    double acc = w[0].x + ((x & 1) ? -w[np].x : w[np].x);
+    for (int kx = 1; kx < np; ++kx) {
+      const int m = (kx * x) % n;
+      acc += 2.0 * (w[kx].x * cs[m] - w[kx].y * sn[m]);
+    }
+    p.plnout[(size_t)node * p.P + s] = acc * inv_g;
+  }
+}
+
+// M2L Hadamard accumulation over sibling groups.  A group is the 8 children
+// of one parent; their V lists all lie in the 6x6x6 window of same-depth
+// positions 2*parent + [-2,3]^3 (fmm/input.cc:311-339), each member taking
+// the window entries at Chebyshev distance >= 2 from itself.  Window entry w
+// = (wx + 6 wy + 36 wz); member c = 4 cx + 2 cy + cz; offset delta = w - 2 -
+// (cx,cy,cz) selects translation spectrum (dx+3) + 7 (dy+3) + 49 (dz+3)
+// (fmm/omp_sse_block.cc:581-593).
+struct HadamardParams {
+  int F;
+  const int* win;     // ngroups x 216 node ids (-1 = absent)
+  const int* members; // ngroups x 8 node ids (-1 = no V list)
+  const double2* trans;  // 343 x F
+  const double2* spec;   // node x F
+  double2* effv;         // node x F
+};
+
+constexpr int kHadThreads = 128;
+
+__global__ void __launch_bounds__(kHadThreads) hadamard_fp64_kernel(HadamardParams p) {
+  __shared__ int win[216];
+  __shared__ int mem[8];
+  const int g = blockIdx.x;
+  for (int w = threadIdx.x; w < 216; w += kHadThreads) win[w] = p.win[(size_t)g * 216 + w];
+  if (threadIdx.x < 8) mem[threadIdx.x] = p.members[(size_t)g * 8 + threadIdx.x];
+  __syncthreads();
+  const int f = blockIdx.y * kHadThreads + threadIdx.x;
+  if (f >= p.F) return;
+  double ar[8], ai[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) ar[c] = ai[c] = 0.0;
+  for (int w = 0; w < 216; ++w) {
+    const int s = win[w];
+    if (s < 0) continue;
+    const double2 S = p.spec[(size_t)s * p.F + f];
+    const int wx = w % 6, wy = (w / 6) % 6, wz = w / 36;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int dx = wx - 2 - (c >> 2), dy = wy - 2 - ((c >> 1) & 1), dz = wz - 2 - (c & 1);
+      const int adx = dx < 0 ? -dx : dx, ady = dy < 0 ? -dy : dy, adz = dz < 0 ? -dz : dz;
+      if (max(adx, max(ady, adz)) < 2 || mem[c] < 0) continue;
+      const double2 T = p.trans[(size_t)((dx + 3) + 7 * (dy + 3) + 49 * (dz + 3)) * p.F + f];
+      ar[c] = fma(T.x, S.x, ar[c]);
+      ar[c] = fma(-T.y, S.y, ar[c]);
+      ai[c] = fma(T.x, S.y, ai[c]);
+      ai[c] = fma(T.y, S.x, ai[c]);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+    if (mem[c] >= 0) p.effv[(size_t)mem[c] * p.F + f] = make_double2(ar[c], ai[c]);
+}
+
+// ---------------------------------------------------------------------------
+// Point reordering (fmm/evaluate.cc:14-52 on the host in the reference) and
+// the final scatter to original order (copy_trg_val, fmm/cuda.cu:2543-2565).
+// ---------------------------------------------------------------------------
+__global__ void gather_points_kernel(int n, const int* perm, const double* x, const double* y,
+                                     const double* z, const double* w, double4* out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int k = perm[i];
+    out[i] = make_double4(x[k], y[k], z[k], w ? w[k] : 0.0);
+  }
+}
+
+__global__ void scatter_pot_kernel(int n, const int* perm, const double* pot_leaf,
+                                   double* pot_orig) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    pot_orig[perm[i]] = pot_leaf[i];
+}
+
+// Plain direct sum (ulist__direct_evaluation) over SoA device arrays.
+__global__ void __launch_bounds__(128) direct_fp64_kernel(int nt, const double* tx,
+                                                          const double* ty, const double* tz,
+                                                          double* pot, int ns, const double* sx,
+                                                          const double* sy, const double* sz,
+                                                          const double* den) {
+  __shared__ double4 stage[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double x = 0, y = 0, z = 0, acc = 0;
+  if (i < nt) {
+    x = tx[i];
+    y = ty[i];
+    z = tz[i];
+  }
+  for (int b = 0; b < ns; b += 256) {
+    const int m = min(256, ns - b);
+    for (int k = threadIdx.x; k < m; k += blockDim.x)
+      stage[k] = make_double4(sx[b + k], sy[b + k], sz[b + k], den[b + k]);
+    __syncthreads();
+    for (int j = 0; j < m; ++j) {
+      const double4 s = stage[j];
+      const double dx = x - s.x, dy = y - s.y, dz = z - s.z;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      acc = fma(s.w, r2 > 0.0 ? rsqrt(r2) : 0.0, acc);
+    }
+    __syncthreads();
+  }
+  if (i < nt) pot[i] += kOOFP * acc;
+}
+
+}  // namespace kfmm

@@ -1,0 +1,876 @@
+// Plan (preproc) and run of the KIFMM evaluator: the C ABI of
+// include/kifmm_b200.h over the kernels of kernels.cuh.
+//
+// Phase order of kfmm_run:
+//   up    : S2M check potentials (P2P) -> UC2UE level GEMM; M2M per level,
+//           deepest first (fmm/cuda.cu:571-600, fmm/omp.cc:61-227)
+//   vlist : forward FFT of every source box, sibling-group Hadamard, inverse
+//           FFT into the downward check potential (fmm/cuda.cu:718-1196)
+//   xlist : S2L onto check surfaces (fmm/cuda.cu:2380-2493)
+//   down  : L2L per level, shallowest first (fmm/cuda.cu:1981-2045)
+//   ulist : one fused kernel per target chunk: U list, W list, direct X list,
+//           and L2T (fmm/cuda.cu:604-663, 2070-2197, 1804-1872)
+//   copy  : potentials back to original order (fmm/cuda.cu:2543-2565)
+// The reference adds U/W/X/L2T contributions into one array in four passes;
+// here each target's potential is summed once in registers and written once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "host.h"
+#include "kernels.cuh"
+
+namespace kfmm {
+
+static thread_local std::string g_error;
+void set_error(const std::string& msg) { g_error = msg; }
+
+#define KF_CUDA(call)                                                               \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                \
+      return KFMM_ERR_CUDA;                                                         \
+    }                                                                               \
+  } while (0)
+
+#define KF_CHECK_LAUNCH(what)                                                       \
+  do {                                                                              \
+    cudaError_t e_ = cudaGetLastError();                                            \
+    if (e_ != cudaSuccess) {                                                        \
+      set_error(std::string(what) + ": " + cudaGetErrorString(e_));                 \
+      return KFMM_ERR_CUDA;                                                         \
+    }                                                                               \
+  } while (0)
+
+struct GemmBatch {
+  const double* A;
+  int M, K;
+  const double* B;
+  int* boff;  // device
+  double* C;
+  int* coff;  // device
+  double* alpha;  // device or null
+  double alpha_const;
+  int ncol;
+  int accumulate;
+};
+
+}  // namespace kfmm
+
+using namespace kfmm;
+
+struct kfmm_plan {
+  int np = 0, P = 0, Q = 0, F = 0, nn = 0, ns = 0, nt = 0, maxdepth = 0;
+  kfmm_precision prec = KFMM_PLAIN_FP64;
+  std::vector<void*> allocs;
+  // tree on device
+  double4* ctr = nullptr;
+  int *d_depth = nullptr, *d_src_beg = nullptr, *d_src_num = nullptr;
+  int *d_src_perm = nullptr, *d_trg_perm = nullptr;
+  // points
+  double *o_sx = nullptr, *o_sy = nullptr, *o_sz = nullptr, *o_w = nullptr;
+  double *o_tx = nullptr, *o_ty = nullptr, *o_tz = nullptr;
+  double4 *src4 = nullptr, *trg4 = nullptr;
+  double *pot_leaf = nullptr, *pot_orig = nullptr;
+  bool have_src = false, have_trg = false;
+  // expansions
+  double *uden = nullptr, *dchk = nullptr, *dden = nullptr, *chk_up = nullptr, *chk_m = nullptr;
+  double2 *spec = nullptr, *effv = nullptr;
+  // operators
+  double *d_uc2ue = nullptr, *d_ue2uc = nullptr, *d_dc2de = nullptr, *d_de2dc_stack = nullptr;
+  double2* d_trans = nullptr;
+  double *d_sp_ue = nullptr, *d_sp_uc = nullptr, *d_sp_de = nullptr, *d_sp_dc = nullptr;
+  double *d_cs = nullptr, *d_sn = nullptr;
+  int *d_surf_idx = nullptr, *d_surf_ijk = nullptr;
+  // work lists
+  P2PJob *s2m_jobs = nullptr, *nf_jobs = nullptr, *s2l_jobs = nullptr;
+  int *s2m_ent = nullptr, *nf_ent = nullptr, *s2l_ent = nullptr;
+  int n_s2m = 0, n_nf = 0, n_s2l = 0;
+  std::vector<GemmBatch> up_gemms, down_gemms;
+  int *fft_nodes = nullptr, *ifft_nodes = nullptr;
+  int n_fft = 0, n_ifft = 0;
+  int *win = nullptr, *members = nullptr;
+  int n_groups = 0;
+  size_t ifft_smem = 0;
+  kfmm_stats stats{};
+  bool timing = false;
+  cudaEvent_t ev[7] = {};
+  float phase_ms[6] = {};
+};
+
+namespace {
+
+template <class T>
+kfmm_status dalloc(kfmm_plan* p, T** ptr, size_t count) {
+  *ptr = nullptr;
+  if (count == 0) count = 1;
+  void* v = nullptr;
+  cudaError_t e = cudaMalloc(&v, count * sizeof(T));
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return KFMM_ERR_ALLOC;
+  }
+  p->allocs.push_back(v);
+  *ptr = (T*)v;
+  return KFMM_OK;
+}
+
+template <class T>
+kfmm_status upload(kfmm_plan* p, T** ptr, const std::vector<T>& h) {
+  kfmm_status s = dalloc(p, ptr, h.size());
+  if (s != KFMM_OK) return s;
+  if (!h.empty()) KF_CUDA(cudaMemcpy(*ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return KFMM_OK;
+}
+
+#define KF_TRY(x)                  \
+  do {                             \
+    kfmm_status s_ = (x);          \
+    if (s_ != KFMM_OK) return s_;  \
+  } while (0)
+
+kfmm_status add_gemm(kfmm_plan* p, std::vector<GemmBatch>& out, const double* A, int M, int K,
+                     const double* B, const std::vector<int>& boff, double* C,
+                     const std::vector<int>& coff, const std::vector<double>* alpha,
+                     double alpha_const, int accumulate) {
+  if (boff.empty()) return KFMM_OK;
+  GemmBatch g{};
+  g.A = A;
+  g.M = M;
+  g.K = K;
+  g.B = B;
+  g.C = C;
+  g.ncol = (int)boff.size();
+  g.accumulate = accumulate;
+  g.alpha_const = alpha_const;
+  KF_TRY(upload(p, &g.boff, boff));
+  KF_TRY(upload(p, &g.coff, coff));
+  if (alpha) KF_TRY(upload(p, &g.alpha, *alpha));
+  p->stats.gemm_flops += 2.0 * M * (double)K * g.ncol;
+  out.push_back(g);
+  return KFMM_OK;
+}
+
+kfmm_status launch_gemms(const std::vector<GemmBatch>& gs, size_t first, size_t last,
+                         cudaStream_t st) {
+  for (size_t i = first; i < last; ++i) {
+    const GemmBatch& b = gs[i];
+    GemmArgs a{b.A, b.M, b.K, b.B, b.boff, b.C, b.coff, b.alpha, b.alpha_const, b.ncol,
+               b.accumulate};
+    dim3 grid((b.M + kGemmBM - 1) / kGemmBM, (b.ncol + kGemmBN - 1) / kGemmBN);
+    gemm_fp64_dmma_kernel<<<grid, 128, 0, st>>>(a);
+    KF_CHECK_LAUNCH("gemm_fp64_dmma_kernel");
+  }
+  return KFMM_OK;
+}
+
+P2PParams p2p_params(const kfmm_plan* p, const P2PJob* jobs, const int* ent, double* out) {
+  P2PParams q;
+  q.jobs = jobs;
+  q.entries = ent;
+  q.src4 = p->src4;
+  q.trg4 = p->trg4;
+  q.ctr = p->ctr;
+  q.src_beg = p->d_src_beg;
+  q.src_num = p->d_src_num;
+  q.uden = p->uden;
+  q.dden = p->dden;
+  q.sp_ue = p->d_sp_ue;
+  q.sp_uc = p->d_sp_uc;
+  q.sp_de = p->d_sp_de;
+  q.sp_dc = p->d_sp_dc;
+  q.out = out;
+  q.P = p->P;
+  q.Q = p->Q;
+  return q;
+}
+
+FFTParams fft_params(const kfmm_plan* p) {
+  FFTParams f{};
+  f.np = p->np;
+  f.P = p->P;
+  f.F = p->F;
+  f.depth = p->d_depth;
+  f.surf_idx = p->d_surf_idx;
+  f.surf_ijk = p->d_surf_ijk;
+  f.cs = p->d_cs;
+  f.sn = p->d_sn;
+  return f;
+}
+
+kfmm_status validate_desc(const kfmm_tree_desc* d) {
+  if (!d || d->num_nodes <= 0 || d->num_src <= 0 || d->num_trg <= 0 || !d->parent || !d->child ||
+      !d->depth || !d->tag || !d->path || !d->src_beg || !d->src_num || !d->trg_beg ||
+      !d->trg_num || !d->src_perm || !d->trg_perm || !d->u_ptr || !d->u_idx || !d->v_ptr ||
+      !d->v_idx || !d->w_ptr || !d->w_idx || !d->x_ptr || !d->x_idx) {
+    set_error("kfmm_plan_create: incomplete tree description");
+    return KFMM_ERR_INVALID;
+  }
+  const int nn = d->num_nodes;
+  for (int i = 0; i < nn; ++i) {
+    if (d->child[i] != -1 && (d->child[i] <= i || d->child[i] + 8 > nn)) {
+      set_error("kfmm_plan_create: child index out of range");
+      return KFMM_ERR_INVALID;
+    }
+    if (d->depth[i] < 0 || d->depth[i] > 20) {
+      set_error("kfmm_plan_create: depth out of range");
+      return KFMM_ERR_INVALID;
+    }
+    if (d->child[i] == -1) {
+      if (d->src_num[i] < 0 || d->src_beg[i] < 0 || d->src_beg[i] + d->src_num[i] > d->num_src ||
+          d->trg_num[i] < 0 || d->trg_beg[i] < 0 || d->trg_beg[i] + d->trg_num[i] > d->num_trg) {
+        set_error("kfmm_plan_create: leaf point range out of bounds");
+        return KFMM_ERR_INVALID;
+      }
+    }
+  }
+  const int* ptrs[4] = {d->u_ptr, d->v_ptr, d->w_ptr, d->x_ptr};
+  const int* idxs[4] = {d->u_idx, d->v_idx, d->w_idx, d->x_idx};
+  for (int k = 0; k < 4; ++k) {
+    if (ptrs[k][0] != 0) {
+      set_error("kfmm_plan_create: list pointer must start at 0");
+      return KFMM_ERR_INVALID;
+    }
+    for (int i = 0; i < nn; ++i)
+      if (ptrs[k][i + 1] < ptrs[k][i]) {
+        set_error("kfmm_plan_create: list pointers not monotone");
+        return KFMM_ERR_INVALID;
+      }
+    for (int j = 0; j < ptrs[k][nn]; ++j)
+      if (idxs[k][j] < 0 || idxs[k][j] >= nn) {
+        set_error("kfmm_plan_create: list entry out of range");
+        return KFMM_ERR_INVALID;
+      }
+  }
+  for (int i = 0; i < d->num_src; ++i)
+    if (d->src_perm[i] < 0 || d->src_perm[i] >= d->num_src) {
+      set_error("kfmm_plan_create: source permutation out of range");
+      return KFMM_ERR_INVALID;
+    }
+  for (int i = 0; i < d->num_trg; ++i)
+    if (d->trg_perm[i] < 0 || d->trg_perm[i] >= d->num_trg) {
+      set_error("kfmm_plan_create: target permutation out of range");
+      return KFMM_ERR_INVALID;
+    }
+  return KFMM_OK;
+}
+
+inline long long key_of(int depth, int x, int y, int z) {
+  return ((long long)depth << 60) | ((long long)x << 40) | ((long long)y << 20) | (long long)z;
+}
+
+kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d) {
+  const int nn = d->num_nodes, np = p->np;
+  const Operators& op = operators_for(np);
+  Surfaces S;
+  make_surfaces(np, &S);
+  const int P = S.P, Q = S.Q, F = S.F;
+  p->P = P;
+  p->Q = Q;
+  p->F = F;
+  p->nn = nn;
+  p->ns = d->num_src;
+  p->nt = d->num_trg;
+  auto is_leaf = [&](int i) { return d->child[i] == -1; };
+  auto has_src = [&](int i) { return (d->tag[i] & kSrcTag) != 0; };
+  auto has_trg = [&](int i) { return (d->tag[i] & kTrgTag) != 0; };
+  int maxd = 0;
+  for (int i = 0; i < nn; ++i) maxd = std::max(maxd, d->depth[i]);
+  p->maxdepth = maxd;
+
+  // --- tree arrays
+  std::vector<double4> ctr(nn);
+  for (int i = 0; i < nn; ++i) {
+    double c[3];
+    for (int k = 0; k < 3; ++k) c[k] = -1.0 + (2.0 * 1.0) * (d->path[3 * i + k] + 0.5) / double(1 << d->depth[i]);
+    ctr[i] = make_double4(c[0], c[1], c[2], 1.0 / double(1 << d->depth[i]));
+  }
+  KF_TRY(upload(p, &p->ctr, ctr));
+  KF_TRY(upload(p, &p->d_depth, std::vector<int>(d->depth, d->depth + nn)));
+  KF_TRY(upload(p, &p->d_src_beg, std::vector<int>(d->src_beg, d->src_beg + nn)));
+  KF_TRY(upload(p, &p->d_src_num, std::vector<int>(d->src_num, d->src_num + nn)));
+  KF_TRY(upload(p, &p->d_src_perm, std::vector<int>(d->src_perm, d->src_perm + d->num_src)));
+  KF_TRY(upload(p, &p->d_trg_perm, std::vector<int>(d->trg_perm, d->trg_perm + d->num_trg)));
+
+  // --- operators and surfaces
+  KF_TRY(upload(p, &p->d_uc2ue, op.uc2ue));
+  KF_TRY(upload(p, &p->d_ue2uc, op.ue2uc));  // Q x 8P, the 8 blocks side by side
+  KF_TRY(upload(p, &p->d_dc2de, op.dc2de));
+  {
+    std::vector<double> st((size_t)8 * P * P);  // 8P x P: the 8 blocks stacked
+    for (int c = 0; c < 8; ++c)
+      for (int j = 0; j < P; ++j)
+        for (int i = 0; i < P; ++i)
+          st[(size_t)j * 8 * P + c * P + i] = op.de2dc[(size_t)c * P * P + (size_t)j * P + i];
+    KF_TRY(upload(p, &p->d_de2dc_stack, st));
+  }
+  {
+    std::vector<double2> tr((size_t)343 * F);
+    for (size_t i = 0; i < tr.size(); ++i) tr[i] = make_double2(op.ue2dc[2 * i], op.ue2dc[2 * i + 1]);
+    KF_TRY(upload(p, &p->d_trans, tr));
+  }
+  KF_TRY(upload(p, &p->d_sp_ue, S.ue));
+  KF_TRY(upload(p, &p->d_sp_uc, S.uc));
+  KF_TRY(upload(p, &p->d_sp_de, S.de));
+  KF_TRY(upload(p, &p->d_sp_dc, S.dc));
+  {
+    const int n = 2 * np;
+    std::vector<double> cs(n), sn(n);
+    for (int m = 0; m < n; ++m) {
+      cs[m] = std::cos(2.0 * M_PI * m / n);
+      sn[m] = std::sin(2.0 * M_PI * m / n);
+    }
+    KF_TRY(upload(p, &p->d_cs, cs));
+    KF_TRY(upload(p, &p->d_sn, sn));
+    std::vector<int> sidx(np * np * np, -1), sijk;
+    int cnt = 0;
+    for (int i = 0; i < np; i++)
+      for (int j = 0; j < np; j++)
+        for (int k = 0; k < np; k++)
+          if (i == 0 || i == np - 1 || j == 0 || j == np - 1 || k == 0 || k == np - 1) {
+            sidx[(i * np + j) * np + k] = cnt++;
+            sijk.push_back(i);
+            sijk.push_back(j);
+            sijk.push_back(k);
+          }
+    KF_TRY(upload(p, &p->d_surf_idx, sidx));
+    KF_TRY(upload(p, &p->d_surf_ijk, sijk));
+  }
+
+  // --- work arrays
+  KF_TRY(dalloc(p, &p->o_sx, p->ns));
+  KF_TRY(dalloc(p, &p->o_sy, p->ns));
+  KF_TRY(dalloc(p, &p->o_sz, p->ns));
+  KF_TRY(dalloc(p, &p->o_w, p->ns));
+  KF_TRY(dalloc(p, &p->o_tx, p->nt));
+  KF_TRY(dalloc(p, &p->o_ty, p->nt));
+  KF_TRY(dalloc(p, &p->o_tz, p->nt));
+  KF_TRY(dalloc(p, &p->src4, p->ns));
+  KF_TRY(dalloc(p, &p->trg4, p->nt));
+  KF_TRY(dalloc(p, &p->pot_leaf, p->nt));
+  KF_TRY(dalloc(p, &p->pot_orig, p->nt));
+  KF_TRY(dalloc(p, &p->uden, (size_t)nn * P));
+  KF_TRY(dalloc(p, &p->dchk, (size_t)nn * P));
+  KF_TRY(dalloc(p, &p->dden, (size_t)nn * P));
+  KF_TRY(dalloc(p, &p->spec, (size_t)nn * F));
+  KF_TRY(dalloc(p, &p->effv, (size_t)nn * F));
+  KF_CUDA(cudaMemset(p->uden, 0, sizeof(double) * (size_t)nn * P));
+  KF_CUDA(cudaMemset(p->dden, 0, sizeof(double) * (size_t)nn * P));
+  KF_CUDA(cudaMemset(p->dchk, 0, sizeof(double) * (size_t)nn * P));
+  KF_CUDA(cudaMemset(p->spec, 0, sizeof(double2) * (size_t)nn * F));
+  KF_CUDA(cudaMemset(p->effv, 0, sizeof(double2) * (size_t)nn * F));
+
+  auto add_chunks = [&](std::vector<P2PJob>& jobs, int tnode, int tkind, int tbeg0, int tcount,
+                        int ebeg, int eend, int out0, int mode) {
+    for (int c = 0; c < tcount; c += kP2PThreads) {
+      P2PJob j;
+      j.tnode = tnode;
+      j.tkind = tkind;
+      j.tbeg = tbeg0 + c;
+      j.tcnt = std::min(kP2PThreads, tcount - c);
+      j.ebeg = ebeg;
+      j.eend = eend;
+      j.out = out0 + c;
+      j.mode = mode;
+      jobs.push_back(j);
+    }
+  };
+  auto src_count = [&](int ent) -> int {
+    int kind = ent >> 28, node = ent & 0x0fffffff;
+    return kind == 0 ? d->src_num[node] : P;
+  };
+
+  // --- up: S2M jobs + UC2UE GEMM, then M2M per level
+  {
+    std::vector<P2PJob> jobs;
+    std::vector<int> ent, boff, coff;
+    std::vector<double> alpha;
+    int slot = 0;
+    for (int i = 0; i < nn; ++i) {
+      if (!is_leaf(i) || !has_src(i)) continue;
+      int e = (int)ent.size();
+      ent.push_back(i);
+      add_chunks(jobs, i, 1, 0, Q, e, e + 1, slot * Q, 0);
+      p->stats.s2m_pairs += (double)Q * d->src_num[i];
+      boff.push_back(slot * Q);
+      coff.push_back(i * P);
+      alpha.push_back(std::ldexp(1.0, -d->depth[i]));
+      ++slot;
+    }
+    p->n_s2m = (int)jobs.size();
+    KF_TRY(upload(p, &p->s2m_jobs, jobs));
+    KF_TRY(upload(p, &p->s2m_ent, ent));
+    KF_TRY(dalloc(p, &p->chk_up, (size_t)std::max(slot, 1) * Q));
+    KF_TRY(add_gemm(p, p->up_gemms, p->d_uc2ue, P, Q, p->chk_up, boff, p->uden, coff, &alpha, 0, 0));
+    int maxpar = 1;
+    std::vector<std::vector<int>> par(maxd + 1);
+    for (int i = 0; i < nn; ++i)
+      if (!is_leaf(i) && has_src(i)) par[d->depth[i]].push_back(i);
+    for (int dd = 0; dd <= maxd; ++dd) maxpar = std::max(maxpar, (int)par[dd].size());
+    KF_TRY(dalloc(p, &p->chk_m, (size_t)maxpar * Q));
+    for (int dd = maxd - 1; dd >= 0; --dd) {
+      if (par[dd].empty()) continue;
+      std::vector<int> b1, c1, b2, c2;
+      for (size_t k = 0; k < par[dd].size(); ++k) {
+        b1.push_back(d->child[par[dd][k]] * P);
+        c1.push_back((int)k * Q);
+        b2.push_back((int)k * Q);
+        c2.push_back(par[dd][k] * P);
+      }
+      KF_TRY(add_gemm(p, p->up_gemms, p->d_ue2uc, Q, 8 * P, p->uden, b1, p->chk_m, c1, nullptr,
+                      std::ldexp(1.0, dd + 1), 0));
+      KF_TRY(add_gemm(p, p->up_gemms, p->d_uc2ue, P, Q, p->chk_m, b2, p->uden, c2, nullptr,
+                      std::ldexp(1.0, -dd), 0));
+    }
+  }
+
+  // --- V list
+  {
+    std::vector<int> fn, ifn;
+    for (int i = 0; i < nn; ++i)
+      if (has_src(i) && d->depth[i] >= 2) fn.push_back(i);
+    for (int i = 0; i < nn; ++i)
+      if (has_trg(i) && d->v_ptr[i + 1] > d->v_ptr[i]) ifn.push_back(i);
+    p->n_fft = (int)fn.size();
+    p->n_ifft = (int)ifn.size();
+    KF_TRY(upload(p, &p->fft_nodes, fn));
+    KF_TRY(upload(p, &p->ifft_nodes, ifn));
+    std::unordered_map<long long, int> at;
+    at.reserve((size_t)nn * 2);
+    for (int i = 0; i < nn; ++i)
+      at[key_of(d->depth[i], d->path[3 * i], d->path[3 * i + 1], d->path[3 * i + 2])] = i;
+    std::vector<int> win, mem;
+    for (int pn = 0; pn < nn; ++pn) {
+      if (is_leaf(pn)) continue;
+      int m[8], any = 0;
+      for (int c = 0; c < 8; ++c) {
+        int ch = d->child[pn] + c;
+        m[c] = (has_trg(ch) && d->v_ptr[ch + 1] > d->v_ptr[ch]) ? ch : -1;
+        any |= m[c] >= 0;
+      }
+      if (!any) continue;
+      const int cd = d->depth[pn] + 1, lim = 1 << cd;
+      int w[216];
+      for (int wz = 0; wz < 6; ++wz)
+        for (int wy = 0; wy < 6; ++wy)
+          for (int wx = 0; wx < 6; ++wx) {
+            int x = 2 * d->path[3 * pn] - 2 + wx, y = 2 * d->path[3 * pn + 1] - 2 + wy,
+                z = 2 * d->path[3 * pn + 2] - 2 + wz;
+            int id = -1;
+            if (x >= 0 && y >= 0 && z >= 0 && x < lim && y < lim && z < lim) {
+              auto it = at.find(key_of(cd, x, y, z));
+              if (it != at.end() && has_src(it->second)) id = it->second;
+            }
+            w[wx + 6 * wy + 36 * wz] = id;
+          }
+      // The window must reproduce every member's V list exactly.
+      for (int c = 0; c < 8; ++c) {
+        if (m[c] < 0) continue;
+        std::vector<int> fromwin;
+        for (int q = 0; q < 216; ++q) {
+          int dx = q % 6 - 2 - (c >> 2), dy = (q / 6) % 6 - 2 - ((c >> 1) & 1), dz = q / 36 - 2 - (c & 1);
+          if (std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz))) >= 2 && w[q] >= 0)
+            fromwin.push_back(w[q]);
+        }
+        std::sort(fromwin.begin(), fromwin.end());
+        std::vector<int> vl(d->v_idx + d->v_ptr[m[c]], d->v_idx + d->v_ptr[m[c] + 1]);
+        std::sort(vl.begin(), vl.end());
+        if (fromwin != vl) {
+          set_error("kfmm_plan_create: V list of node " + std::to_string(m[c]) +
+                    " is not the same-depth far part of its parent's neighbourhood");
+          return KFMM_ERR_INVALID;
+        }
+        p->stats.v_pairs += (double)vl.size();
+        p->stats.hadamard_cmacs += (double)vl.size() * F;
+      }
+      win.insert(win.end(), w, w + 216);
+      mem.insert(mem.end(), m, m + 8);
+    }
+    p->n_groups = (int)mem.size() / 8;
+    KF_TRY(upload(p, &p->win, win));
+    KF_TRY(upload(p, &p->members, mem));
+    p->stats.spectra_bytes = 16.0 * F * ((double)fn.size() + (double)ifn.size());
+  }
+
+  // --- X list S2L jobs
+  {
+    std::vector<P2PJob> jobs;
+    std::vector<int> ent;
+    for (int t = 0; t < nn; ++t) {
+      if (!has_trg(t)) continue;
+      int xb = d->x_ptr[t], xe = d->x_ptr[t + 1];
+      if (xe == xb) continue;
+      if (is_leaf(t) && d->trg_num[t] < P) continue;  // handled directly in the near field
+      int e0 = (int)ent.size();
+      int ns = 0;
+      for (int k = xb; k < xe; ++k) {
+        ent.push_back(d->x_idx[k]);
+        ns += d->src_num[d->x_idx[k]];
+      }
+      add_chunks(jobs, t, 2, 0, P, e0, (int)ent.size(), t * P, 1);
+      p->stats.s2l_pairs += (double)P * ns;
+    }
+    p->n_s2l = (int)jobs.size();
+    KF_TRY(upload(p, &p->s2l_jobs, jobs));
+    KF_TRY(upload(p, &p->s2l_ent, ent));
+  }
+
+  // --- down: L2L per level
+  for (int dd = 2; dd <= maxd; ++dd) {
+    if (dd >= 3) {
+      std::vector<int> b1, c1;
+      for (int i = 0; i < nn; ++i)
+        if (d->depth[i] == dd - 1 && !is_leaf(i) && has_trg(i)) {
+          b1.push_back(i * P);
+          c1.push_back(d->child[i] * P);
+        }
+      KF_TRY(add_gemm(p, p->down_gemms, p->d_de2dc_stack, 8 * P, P, p->dden, b1, p->dchk, c1,
+                      nullptr, std::ldexp(1.0, dd - 1), 1));
+    }
+    std::vector<int> b2;
+    for (int i = 0; i < nn; ++i)
+      if (d->depth[i] == dd && has_trg(i)) b2.push_back(i * P);
+    KF_TRY(add_gemm(p, p->down_gemms, p->d_dc2de, P, P, p->dchk, b2, p->dden, b2, nullptr,
+                    std::ldexp(1.0, -dd), 0));
+  }
+
+  // --- near field: U + W + direct X + L2T
+  {
+    std::vector<P2PJob> jobs;
+    std::vector<int> ent;
+    for (int t = 0; t < nn; ++t) {
+      if (!is_leaf(t) || !has_trg(t) || d->trg_num[t] == 0) continue;
+      int e0 = (int)ent.size();
+      for (int k = d->u_ptr[t]; k < d->u_ptr[t + 1]; ++k) ent.push_back(d->u_idx[k]);
+      for (int k = d->w_ptr[t]; k < d->w_ptr[t + 1]; ++k) {
+        int s = d->w_idx[k];
+        bool direct = is_leaf(s) && d->src_num[s] < P;  // fmm/omp.cc:675
+        ent.push_back(direct ? s : ((1 << 28) | s));
+      }
+      if (d->trg_num[t] < P)  // fmm/omp.cc:724
+        for (int k = d->x_ptr[t]; k < d->x_ptr[t + 1]; ++k) ent.push_back(d->x_idx[k]);
+      if (d->depth[t] >= 2) ent.push_back((2 << 28) | t);
+      int ns = 0;
+      for (int k = e0; k < (int)ent.size(); ++k) ns += src_count(ent[k]);
+      add_chunks(jobs, t, 0, d->trg_beg[t], d->trg_num[t], e0, (int)ent.size(), d->trg_beg[t], 0);
+      p->stats.u_pairs += (double)d->trg_num[t] * ns;
+    }
+    p->n_nf = (int)jobs.size();
+    KF_TRY(upload(p, &p->nf_jobs, jobs));
+    KF_TRY(upload(p, &p->nf_ent, ent));
+  }
+
+  p->ifft_smem = sizeof(double2) * ((size_t)F + (size_t)np * 2 * np * (np + 1));
+  KF_CUDA(cudaFuncSetAttribute(ifft_trg_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)p->ifft_smem));
+  p->stats.num_nodes = nn;
+  p->stats.P = P;
+  p->stats.Q = Q;
+  p->stats.F = F;
+  p->stats.launches = (p->n_s2m > 0) + (int)p->up_gemms.size() + (p->n_fft > 0) +
+                      (p->n_groups > 0) + (p->n_ifft > 0) + (p->n_s2l > 0) +
+                      (int)p->down_gemms.size() + (p->n_nf > 0) + 1;
+  for (int i = 0; i < 7; ++i) KF_CUDA(cudaEventCreate(&p->ev[i]));
+  return KFMM_OK;
+}
+
+inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+
+void mark(kfmm_plan* p, int i, cudaStream_t st) {
+  if (p->timing) cudaEventRecord(p->ev[i], st);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* kfmm_last_error(void) { return g_error.c_str(); }
+const char* kfmm_version(void) { return "kifmm_b200 0.1 (sm_100a)"; }
+
+kfmm_status kfmm_plan_create(const kfmm_tree_desc* tree, int np, kfmm_precision precision,
+                             kfmm_plan** out) {
+  if (!out) {
+    set_error("kfmm_plan_create: out is NULL");
+    return KFMM_ERR_INVALID;
+  }
+  *out = nullptr;
+  if (np < 3 || np > 8) {
+    set_error("kfmm_plan_create: NP must be in 3..8");
+    return KFMM_ERR_UNSUPPORTED;
+  }
+  if (precision != KFMM_PLAIN_FP64 && precision != KFMM_MIXED) {
+    set_error("kfmm_plan_create: unknown precision");
+    return KFMM_ERR_INVALID;
+  }
+  KF_TRY(validate_desc(tree));
+  kfmm_plan* p = new kfmm_plan();
+  p->np = np;
+  p->prec = precision;
+  kfmm_status s = build_plan(p, tree);
+  if (s != KFMM_OK) {
+    std::string keep = g_error;
+    kfmm_plan_destroy(p);
+    g_error = keep;
+    return s;
+  }
+  *out = p;
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_plan_destroy(kfmm_plan* p) {
+  if (!p) return KFMM_OK;
+  for (void* v : p->allocs) cudaFree(v);
+  for (int i = 0; i < 7; ++i)
+    if (p->ev[i]) cudaEventDestroy(p->ev[i]);
+  delete p;
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_set_sources_device(kfmm_plan* p, const double* sx, const double* sy,
+                                    const double* sz, const double* den, void* stream) {
+  if (!p || !sx || !sy || !sz || !den) {
+    set_error("kfmm_set_sources_device: null argument");
+    return KFMM_ERR_INVALID;
+  }
+  gather_points_kernel<<<592, 256, 0, S(stream)>>>(p->ns, p->d_src_perm, sx, sy, sz, den, p->src4);
+  KF_CHECK_LAUNCH("gather_points_kernel");
+  p->have_src = true;
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_set_targets_device(kfmm_plan* p, const double* tx, const double* ty,
+                                    const double* tz, void* stream) {
+  if (!p || !tx || !ty || !tz) {
+    set_error("kfmm_set_targets_device: null argument");
+    return KFMM_ERR_INVALID;
+  }
+  gather_points_kernel<<<592, 256, 0, S(stream)>>>(p->nt, p->d_trg_perm, tx, ty, tz, nullptr, p->trg4);
+  KF_CHECK_LAUNCH("gather_points_kernel");
+  p->have_trg = true;
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_set_sources(kfmm_plan* p, const double* sx, const double* sy, const double* sz,
+                             const double* den, void* stream) {
+  if (!p || !sx || !sy || !sz || !den) {
+    set_error("kfmm_set_sources: null argument");
+    return KFMM_ERR_INVALID;
+  }
+  const size_t b = sizeof(double) * p->ns;
+  KF_CUDA(cudaMemcpyAsync(p->o_sx, sx, b, cudaMemcpyHostToDevice, S(stream)));
+  KF_CUDA(cudaMemcpyAsync(p->o_sy, sy, b, cudaMemcpyHostToDevice, S(stream)));
+  KF_CUDA(cudaMemcpyAsync(p->o_sz, sz, b, cudaMemcpyHostToDevice, S(stream)));
+  KF_CUDA(cudaMemcpyAsync(p->o_w, den, b, cudaMemcpyHostToDevice, S(stream)));
+  return kfmm_set_sources_device(p, p->o_sx, p->o_sy, p->o_sz, p->o_w, stream);
+}
+
+kfmm_status kfmm_set_targets(kfmm_plan* p, const double* tx, const double* ty, const double* tz,
+                             void* stream) {
+  if (!p || !tx || !ty || !tz) {
+    set_error("kfmm_set_targets: null argument");
+    return KFMM_ERR_INVALID;
+  }
+  const size_t b = sizeof(double) * p->nt;
+  KF_CUDA(cudaMemcpyAsync(p->o_tx, tx, b, cudaMemcpyHostToDevice, S(stream)));
+  KF_CUDA(cudaMemcpyAsync(p->o_ty, ty, b, cudaMemcpyHostToDevice, S(stream)));
+  KF_CUDA(cudaMemcpyAsync(p->o_tz, tz, b, cudaMemcpyHostToDevice, S(stream)));
+  return kfmm_set_targets_device(p, p->o_tx, p->o_ty, p->o_tz, stream);
+}
+
+kfmm_status kfmm_up_calc(kfmm_plan* p, void* stream) {
+  if (!p || !p->have_src) {
+    set_error("kfmm_up_calc: plan has no sources");
+    return KFMM_ERR_STATE;
+  }
+  if (p->n_s2m) {
+    p2p_fp64_kernel<<<p->n_s2m, kP2PThreads, 0, S(stream)>>>(
+        p2p_params(p, p->s2m_jobs, p->s2m_ent, p->chk_up));
+    KF_CHECK_LAUNCH("p2p_fp64_kernel(s2m)");
+  }
+  return launch_gemms(p->up_gemms, 0, p->up_gemms.size(), S(stream));
+}
+
+kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
+  if (!p) return KFMM_ERR_INVALID;
+  KF_CUDA(cudaMemsetAsync(p->dchk, 0, sizeof(double) * (size_t)p->nn * p->P, S(stream)));
+  FFTParams f = fft_params(p);
+  if (p->n_fft) {
+    f.nodes = p->fft_nodes;
+    f.pln = p->uden;
+    f.specout = p->spec;
+    fft_src_fp64_kernel<<<p->n_fft, kFFTThreads, 0, S(stream)>>>(f);
+    KF_CHECK_LAUNCH("fft_src_fp64_kernel");
+  }
+  if (p->n_groups) {
+    HadamardParams h{p->F, p->win, p->members, p->d_trans, p->spec, p->effv};
+    dim3 grid(p->n_groups, (p->F + kHadThreads - 1) / kHadThreads);
+    hadamard_fp64_kernel<<<grid, kHadThreads, 0, S(stream)>>>(h);
+    KF_CHECK_LAUNCH("hadamard_fp64_kernel");
+  }
+  if (p->n_ifft) {
+    f.nodes = p->ifft_nodes;
+    f.specin = p->effv;
+    f.plnout = p->dchk;
+    ifft_trg_fp64_kernel<<<p->n_ifft, kFFTThreads, p->ifft_smem, S(stream)>>>(f);
+    KF_CHECK_LAUNCH("ifft_trg_fp64_kernel");
+  }
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_xlist_calc(kfmm_plan* p, void* stream) {
+  if (!p) return KFMM_ERR_INVALID;
+  if (p->n_s2l) {
+    p2p_fp64_kernel<<<p->n_s2l, kP2PThreads, 0, S(stream)>>>(
+        p2p_params(p, p->s2l_jobs, p->s2l_ent, p->dchk));
+    KF_CHECK_LAUNCH("p2p_fp64_kernel(s2l)");
+  }
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_down_calc(kfmm_plan* p, void* stream) {
+  if (!p) return KFMM_ERR_INVALID;
+  return launch_gemms(p->down_gemms, 0, p->down_gemms.size(), S(stream));
+}
+
+kfmm_status kfmm_ulist_calc(kfmm_plan* p, void* stream) {
+  if (!p || !p->have_trg || !p->have_src) {
+    set_error("kfmm_ulist_calc: plan has no points");
+    return KFMM_ERR_STATE;
+  }
+  if (p->n_nf) {
+    p2p_fp64_kernel<<<p->n_nf, kP2PThreads, 0, S(stream)>>>(
+        p2p_params(p, p->nf_jobs, p->nf_ent, p->pot_leaf));
+    KF_CHECK_LAUNCH("p2p_fp64_kernel(near field)");
+  }
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_copy_trg_val(kfmm_plan* p, double* pot_host, void* stream) {
+  if (!p) return KFMM_ERR_INVALID;
+  scatter_pot_kernel<<<592, 256, 0, S(stream)>>>(p->nt, p->d_trg_perm, p->pot_leaf, p->pot_orig);
+  KF_CHECK_LAUNCH("scatter_pot_kernel");
+  if (pot_host) {
+    KF_CUDA(cudaMemcpyAsync(pot_host, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToHost,
+                            S(stream)));
+    KF_CUDA(cudaStreamSynchronize(S(stream)));
+  }
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_get_potentials_device(kfmm_plan* p, double* pot_dev, void* stream) {
+  if (!p || !pot_dev) return KFMM_ERR_INVALID;
+  KF_CUDA(cudaMemcpyAsync(pot_dev, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToDevice,
+                          S(stream)));
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_run(kfmm_plan* p, void* stream) {
+  if (!p) {
+    set_error("kfmm_run: null plan");
+    return KFMM_ERR_INVALID;
+  }
+  if (!p->have_src || !p->have_trg) {
+    set_error("kfmm_run: set sources and targets first");
+    return KFMM_ERR_STATE;
+  }
+  cudaStream_t st = S(stream);
+  mark(p, 0, st);
+  KF_TRY(kfmm_up_calc(p, stream));
+  mark(p, 1, st);
+  KF_TRY(kfmm_vlist_calc(p, stream));
+  mark(p, 2, st);
+  KF_TRY(kfmm_xlist_calc(p, stream));
+  mark(p, 3, st);
+  KF_TRY(kfmm_down_calc(p, stream));
+  mark(p, 4, st);
+  KF_TRY(kfmm_ulist_calc(p, stream));
+  mark(p, 5, st);
+  KF_TRY(kfmm_copy_trg_val(p, nullptr, stream));
+  mark(p, 6, st);
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_evaluate(kfmm_plan* p, const double* sx, const double* sy, const double* sz,
+                          const double* den, const double* tx, const double* ty,
+                          const double* tz, double* pot, void* stream) {
+  if (!p || !pot) {
+    set_error("kfmm_evaluate: null argument");
+    return KFMM_ERR_INVALID;
+  }
+  KF_TRY(kfmm_set_targets(p, tx, ty, tz, stream));
+  KF_TRY(kfmm_set_sources(p, sx, sy, sz, den, stream));
+  KF_TRY(kfmm_run(p, stream));
+  KF_CUDA(cudaMemcpyAsync(pot, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToHost,
+                          S(stream)));
+  KF_CUDA(cudaStreamSynchronize(S(stream)));
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_direct_evaluation(int nt, const double* tx, const double* ty, const double* tz,
+                                   double* pot, int ns, const double* sx, const double* sy,
+                                   const double* sz, const double* den, void* stream) {
+  if (nt < 0 || ns < 0 || (nt > 0 && (!tx || !ty || !tz || !pot)) ||
+      (ns > 0 && (!sx || !sy || !sz || !den))) {
+    set_error("kfmm_direct_evaluation: bad argument");
+    return KFMM_ERR_INVALID;
+  }
+  if (nt == 0 || ns == 0) return KFMM_OK;
+  direct_fp64_kernel<<<(nt + 127) / 128, 128, 0, S(stream)>>>(nt, tx, ty, tz, pot, ns, sx, sy, sz,
+                                                              den);
+  KF_CHECK_LAUNCH("direct_fp64_kernel");
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_read_array(kfmm_plan* p, int which, double* out, size_t count) {
+  if (!p || !out) return KFMM_ERR_INVALID;
+  const void* src = nullptr;
+  size_t avail = 0;
+  switch (which) {
+    case 0: src = p->uden; avail = (size_t)p->nn * p->P; break;
+    case 1: src = p->dchk; avail = (size_t)p->nn * p->P; break;
+    case 2: src = p->dden; avail = (size_t)p->nn * p->P; break;
+    case 3: src = p->pot_leaf; avail = (size_t)p->nt; break;
+    case 4: src = p->spec; avail = (size_t)p->nn * p->F * 2; break;
+    default:
+      set_error("kfmm_read_array: unknown array");
+      return KFMM_ERR_INVALID;
+  }
+  if (count > avail) {
+    set_error("kfmm_read_array: count exceeds array size");
+    return KFMM_ERR_INVALID;
+  }
+  KF_CUDA(cudaDeviceSynchronize());
+  KF_CUDA(cudaMemcpy(out, src, count * sizeof(double), cudaMemcpyDeviceToHost));
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_plan_stats(const kfmm_plan* p, kfmm_stats* s) {
+  if (!p || !s) return KFMM_ERR_INVALID;
+  *s = p->stats;
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_enable_timing(kfmm_plan* p, int enable) {
+  if (!p) return KFMM_ERR_INVALID;
+  p->timing = enable != 0;
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_phase_times(const kfmm_plan* p, float* ms) {
+  if (!p || !ms) return KFMM_ERR_INVALID;
+  if (!p->timing) {
+    set_error("kfmm_phase_times: timing not enabled");
+    return KFMM_ERR_STATE;
+  }
+  KF_CUDA(cudaEventSynchronize(p->ev[6]));
+  for (int i = 0; i < 6; ++i) KF_CUDA(cudaEventElapsedTime(&ms[i], p->ev[i], p->ev[i + 1]));
+  return KFMM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,48 @@
+/*
+ * Test infrastructure (oracle build only): see mkl.h.
+ */
+#include <assert.h>
+#include <stddef.h>
+
+#include "mkl.h"
+
+/* OpenBLAS (gfortran ABI: hidden string lengths after the argument list) */
+extern void scipy_dgesvd_(const char*, const char*, const int*, const int*, double*,
+                          const int*, double*, double*, const int*, double*,
+                          const int*, double*, const int*, int*, size_t, size_t);
+extern void scipy_dgemm_(const char*, const char*, const int*, const int*, const int*,
+                         const double*, const double*, const int*, const double*,
+                         const int*, const double*, double*, const int*, size_t,
+                         size_t);
+
+void DGESVD(const char* jobu, const char* jobvt, const int* m, const int* n, double* a,
+            const int* lda, double* s, double* u, const int* ldu, double* vt,
+            const int* ldvt, double* work, const int* lwork, int* info) {
+  scipy_dgesvd_(jobu, jobvt, m, n, a, lda, s, u, ldu, vt, ldvt, work, lwork, info, 1,
+                1);
+}
+
+void DGEMM(const char* transa, const char* transb, const int* m, const int* n,
+           const int* k, const double* alpha, const double* a, const int* lda,
+           const double* b, const int* ldb, const double* beta, double* c,
+           const int* ldc) {
+  scipy_dgemm_(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, 1, 1);
+}
+
+void DGEMV(const char* trans, const int* m, const int* n, const double* alpha,
+           const double* a, const int* lda, const double* x, const int* incx,
+           const double* beta, double* y, const int* incy) {
+  assert((*trans == 'N' || *trans == 'n') && *incx == 1 && *incy == 1);
+  const int M = *m, N = *n, LD = *lda;
+  for (int i = 0; i < M; ++i) y[i] *= *beta;
+  for (int j = 0; j < N; ++j) {
+    const double t = *alpha * x[j];
+    const double* col = a + (size_t)j * LD;
+    for (int i = 0; i < M; ++i) y[i] += t * col[i];
+  }
+}
+
+void DAXPY(const int* n, const double* alpha, const double* x, const int* incx,
+           double* y, const int* incy) {
+  for (int i = 0; i < *n; ++i) y[(size_t)i * *incy] += *alpha * x[(size_t)i * *incx];
+}
