@@ -1,0 +1,324 @@
+"""Benchmark: KIFMM 3-D Laplace solve throughput (Mpts/s) on B200.
+
+Workload (one "step" = one full FMM evaluation of a fixed synthetic problem):
+4,194,304 uniform points in [-1,1)^3 (the reference's "uniform" generator,
+srand48(26)), densities in [0,1), NP=6, at most 512 points per leaf.  Tree,
+lists and operators are built once (untimed, like the reference's preproc);
+`value` times kfmm_run with inputs resident in HBM; `e2e` times kfmm_evaluate
+from pinned host buffers (H2D of points and densities, the solve, D2H of the
+potentials).  Multi-GPU runs are replicas (one independent solve per rank,
+weak scaling, no collective on the data path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_POINTS = 4194304
+NP = 6
+PPB = 512
+DIST = "uniform"
+METRIC = "Mpts/s per FMM solve at 4M pts NP=6, mixed vs FP64 on B200, rel-L2 err vs FP64"
+WORKLOAD = "KIFMM Laplace solve, 4194304 uniform points, NP=6, 512 pts/box"
+CPU_SAMPLE_N = 1048576  # bounded sample for the CPU reference (same NP, leaf size, generator)
+FLOPS_PER_PAIR = 11.0   # reference convention, fmm/driver.cc:60
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_POINTS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def run_reference_cpu(n, steps, warmup):
+    """The reference's own blocked-SSE CPU evaluator (fmmd--omp_sse_block,
+    built from its sources into oracle/_ref), all host threads, on a bounded
+    sample of the workload.  Returns (Mpts/s median, per-run seconds, kind)."""
+    import oracle  # noqa: F401  (checker package; only its build lives here)
+    exe = os.path.join(ROOT, "oracle", "_ref", "fmmd--omp_sse_block")
+    if not os.path.exists(exe):
+        return None
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, NP=str(NP), NV="1", OMP_NUM_THREADS=str(cores),
+               GLIBC_TUNABLES="glibc.malloc.mmap_threshold=4096")
+    times = []
+    for i in range(warmup + steps):
+        r = subprocess.run([exe, str(n), DIST, str(PPB)], env=env, capture_output=True,
+                           text=True, timeout=900)
+        m = re.search(r"Total Execution Time:\s*([0-9.eE+-]+)", r.stderr)
+        if r.returncode != 0 or not m:
+            raise RuntimeError("fmmd--omp_sse_block failed: " + r.stderr[-300:])
+        if i >= warmup:
+            times.append(float(m.group(1)))
+    t = statistics.median(times)
+    return {"value": n / t / 1e6, "unit": "Mpts/s", "cores": cores, "kind": "reference",
+            "seconds": times,
+            "sample": f"fmmd--omp_sse_block {n} {DIST} {PPB}, NP={NP}, OMP_NUM_THREADS={cores}; "
+                      "the reference's own 'Total Execution Time' (includes its in-phase "
+                      "operator precompute)"}
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    steps, warmup = max(1, min(args.steps, 5)), max(0, min(args.warmup, 1))
+    res = run_reference_cpu(CPU_SAMPLE_N, steps, warmup)
+    if res is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/fmmd--omp_sse_block not built"}))
+        return
+    v = res["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpts/s",
+            "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
+            "ms_per_step": 1e3 * statistics.median(res["seconds"]), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample_points": CPU_SAMPLE_N, "np": NP,
+                       "pts_per_box": PPB, "distribution": DIST},
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    import __graft_entry__
+
+    K = __graft_entry__.load_package()
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    n = args.n
+
+    # ---- setup (untimed): points, tree + lists, plan (operators, device arrays)
+    pts = K.generate_points(n, DIST, 0, 26 + rank, 1000)
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], PPB)
+    plan = K.Plan(tree, NP, K.PLAIN_FP64)
+    stream = torch.cuda.current_stream(dev)
+    sh = ctypes_stream = stream.cuda_stream
+    plan.set_points(pts, ctypes_stream)
+    st = plan.stats()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        plan.run(sh)
+    torch.cuda.synchronize()
+
+    # ---- timed: K solves, inputs resident in HBM
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.5)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.run(sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n * world / (ms * 1e3)
+
+    # ---- phase breakdown and the dominant kernel timed alone on its stream
+    plan.enable_timing(True)
+    plan.run(sh)
+    phases = plan.phase_times()
+    plan.enable_timing(False)
+    nf_ms = []
+    for _ in range(3):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        K.check(K.lib().kfmm_ulist_calc(plan.handle, sh), "ulist")
+        b.record(stream)
+        torch.cuda.synchronize()
+        nf_ms.append(a.elapsed_time(b))
+    nf = statistics.median(nf_ms)
+    pot = plan.potentials(sh)
+
+    # ---- the reference's check: rel-L2 vs an FP64 direct sum on 1000 targets
+    ids = pts["check_ids"]
+    dsrc = [torch.tensor(pts[k], device=dev) for k in ("sx", "sy", "sz", "den")]
+    dtrg = [torch.tensor(pts[k][ids], device=dev) for k in ("tx", "ty", "tz")]
+    direct = torch.zeros(len(ids), dtype=torch.float64, device=dev)
+    K.check(K.lib().kfmm_direct_evaluation(len(ids), *[x.data_ptr() for x in dtrg],
+                                           direct.data_ptr(), n, *[x.data_ptr() for x in dsrc],
+                                           sh), "direct")
+    torch.cuda.synchronize()
+    direct = direct.cpu().numpy()
+    rel_l2 = float(np.linalg.norm(pot[ids] - direct) / np.linalg.norm(pot[ids]))
+
+    # ---- e2e through the C ABI from pinned host buffers
+    hp = {k: torch.from_numpy(pts[k]).pin_memory() for k in ("sx", "sy", "sz", "den", "tx", "ty",
+                                                           "tz")}
+    hout = torch.empty(n, dtype=torch.float64).pin_memory()
+    ptrs = [hp[k].data_ptr() for k in ("sx", "sy", "sz", "den", "tx", "ty", "tz")]
+    import ctypes
+    fp = ctypes.POINTER(ctypes.c_double)
+    cargs = [ctypes.cast(p_, fp) for p_ in ptrs] + [ctypes.cast(hout.data_ptr(), fp)]
+    K.check(K.lib().kfmm_evaluate(plan.handle, *cargs, sh), "evaluate")
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(e2e_steps):
+        K.check(K.lib().kfmm_evaluate(plan.handle, *cargs, sh), "evaluate")
+    b.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    assert np.array_equal(hout.numpy(), pot), "e2e potentials differ from the resident run"
+
+    peaks = measured_peaks()
+    fp64_peak = float(os.environ.get("KFMM_FP64_PEAK_TFLOPS", "0") or 0) or None
+    achieved = FLOPS_PER_PAIR * st["u_pairs"] / (nf * 1e-3) / 1e12
+    roof = {"bound": "fp64", "kernel": "p2p_fp64_kernel (near field: U+W+X+L2T)",
+            "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+            "frac": (achieved / fp64_peak) if fp64_peak else None, "traffic": None,
+            "algorithmic": f"{FLOPS_PER_PAIR:g} flops/pair x {st['u_pairs']:.4e} pairs per launch",
+            "launch_ms": nf}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            res = run_reference_cpu(CPU_SAMPLE_N, 1, 0)
+            if res:
+                cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "error": str(ex)[:200]}
+
+    h2d = 7 * 8 * n
+    d2h = 8 * n
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_points": n, "np": NP, "pts_per_box": PPB,
+                   "distribution": DIST, "precision": "plain_fp64",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (points 268 MB; expansions and spectra >1 GB)"},
+        "rel_l2_err": rel_l2,
+        "phases_ms": phases,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": n * world / (e2e_ms * 1e3), "unit": "Mpts/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(st["launches"]) * args.steps,
+        "clocks": clk,
+        "tree": {"nodes": st["num_nodes"], "u_pairs": st["u_pairs"], "v_pairs": st["v_pairs"]},
+        "hbm_peak_gbs": peaks.get("hbm_gbs"),
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    plan.close()
+    tree.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -98,6 +98,23 @@ typedef struct kfmm_plan kfmm_plan;
 
 kfmm_status kfmm_plan_create(const kfmm_tree_desc* tree, int np, kfmm_precision precision,
                              kfmm_plan** out);
+
+/* Operator matrices supplied by the caller, layouts as kfmm_operators()
+ * writes them.  The drop-in preproc passes the matrices its own trans.cc
+ * computed (fmm/evaluate--cuda.cu:1628-1643 uploads the same set), so results
+ * do not depend on which LAPACK produced the pseudo-inverses: with kappa ~
+ * 0.1^-(np+1) a different SVD moves the potentials by ~1e-10 (NP=6). */
+typedef struct {
+  const double* uc2ue; /* P x Q */
+  const double* ue2uc; /* 8 x (Q x P) */
+  const double* dc2de; /* P x P */
+  const double* de2dc; /* 8 x (P x P) */
+  const double* ue2dc; /* 343 x F complex; NULL: computed here */
+} kfmm_operator_set;
+
+kfmm_status kfmm_plan_create_with_operators(const kfmm_tree_desc* tree, int np,
+                                            kfmm_precision precision,
+                                            const kfmm_operator_set* ops, kfmm_plan** out);
 kfmm_status kfmm_plan_destroy(kfmm_plan* plan);
 
 /* Points in ORIGINAL order.  Host variants copy host->device inside the call

@@ -39,6 +39,10 @@ class TreeDesc(ctypes.Structure):
                              "x_idx")]
 
 
+class OperatorSet(ctypes.Structure):
+    _fields_ = [(n, _f64p) for n in ("uc2ue", "ue2uc", "dc2de", "de2dc", "ue2dc")]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in ("u_pairs", "s2m_pairs", "s2l_pairs", "v_pairs",
                                                 "hadamard_cmacs", "gemm_flops",
@@ -63,6 +67,8 @@ def lib():
         "kfmm_sizes": [i, _i32p, _i32p, _i32p],
         "kfmm_operators": [i, _f64p, _f64p, _f64p, _f64p, _f64p],
         "kfmm_plan_create": [ctypes.POINTER(TreeDesc), i, i, ctypes.POINTER(vp)],
+        "kfmm_plan_create_with_operators": [ctypes.POINTER(TreeDesc), i, i,
+                                            ctypes.POINTER(OperatorSet), ctypes.POINTER(vp)],
         "kfmm_plan_destroy": [vp],
         "kfmm_set_sources": [vp, _f64p, _f64p, _f64p, _f64p, vp],
         "kfmm_set_targets": [vp, _f64p, _f64p, _f64p, vp],
@@ -172,12 +178,24 @@ class Tree:
 class Plan:
     """An evaluation plan on the current CUDA device."""
 
-    def __init__(self, tree, np_, precision=PLAIN_FP64):
+    def __init__(self, tree, np_, precision=PLAIN_FP64, operators=None):
+        """operators: optional dict (uc2ue, ue2uc, dc2de, de2dc[, ue2dc]) in
+        kfmm_operators layout, e.g. the reference's own matrices."""
         self.tree = tree
         self.np = np_
         h = ctypes.c_void_p()
-        check(lib().kfmm_plan_create(ctypes.byref(tree.desc), np_, precision, ctypes.byref(h)),
-              "plan_create")
+        if operators is None:
+            check(lib().kfmm_plan_create(ctypes.byref(tree.desc), np_, precision,
+                                         ctypes.byref(h)), "plan_create")
+        else:
+            keep = {k: np.ascontiguousarray(operators[k], np.float64)
+                    for k in ("uc2ue", "ue2uc", "dc2de", "de2dc", "ue2dc") if k in operators}
+            null = ctypes.cast(None, _f64p)
+            ops = OperatorSet(*[_p(keep[k]) if k in keep else null
+                                for k in ("uc2ue", "ue2uc", "dc2de", "de2dc", "ue2dc")])
+            check(lib().kfmm_plan_create_with_operators(ctypes.byref(tree.desc), np_, precision,
+                                                        ctypes.byref(ops), ctypes.byref(h)),
+                  "plan_create_with_operators")
         self.handle = h
         self.nt = tree.desc.num_trg
         self.ns = tree.desc.num_src

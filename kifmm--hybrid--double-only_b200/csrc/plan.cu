@@ -207,8 +207,10 @@ FFTParams fft_params(const kfmm_plan* p) {
 kfmm_status validate_desc(const kfmm_tree_desc* d) {
   if (!d || d->num_nodes <= 0 || d->num_src <= 0 || d->num_trg <= 0 || !d->parent || !d->child ||
       !d->depth || !d->tag || !d->path || !d->src_beg || !d->src_num || !d->trg_beg ||
-      !d->trg_num || !d->src_perm || !d->trg_perm || !d->u_ptr || !d->u_idx || !d->v_ptr ||
-      !d->v_idx || !d->w_ptr || !d->w_idx || !d->x_ptr || !d->x_idx) {
+      !d->trg_num || !d->src_perm || !d->trg_perm || !d->u_ptr || !d->v_ptr || !d->w_ptr ||
+      !d->x_ptr || (d->u_ptr[d->num_nodes] > 0 && !d->u_idx) ||
+      (d->v_ptr[d->num_nodes] > 0 && !d->v_idx) || (d->w_ptr[d->num_nodes] > 0 && !d->w_idx) ||
+      (d->x_ptr[d->num_nodes] > 0 && !d->x_idx)) {
     set_error("kfmm_plan_create: incomplete tree description");
     return KFMM_ERR_INVALID;
   }
@@ -261,13 +263,26 @@ kfmm_status validate_desc(const kfmm_tree_desc* d) {
   return KFMM_OK;
 }
 
-inline long long key_of(int depth, int x, int y, int z) {
-  return ((long long)depth << 60) | ((long long)x << 40) | ((long long)y << 20) | (long long)z;
+// Key of a position within one level (coordinates < 2^20 since depth <= 20).
+inline long long key_of(int x, int y, int z) {
+  return (long long)x | ((long long)y << 21) | ((long long)z << 42);
 }
 
-kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d) {
+kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operator_set* user) {
   const int nn = d->num_nodes, np = p->np;
-  const Operators& op = operators_for(np);
+  Operators op = operators_for(np);
+  if (user) {
+    const size_t P0 = op.P, Q0 = op.Q;
+    if (!user->uc2ue || !user->ue2uc || !user->dc2de || !user->de2dc) {
+      set_error("kfmm_plan_create_with_operators: uc2ue, ue2uc, dc2de and de2dc are required");
+      return KFMM_ERR_INVALID;
+    }
+    op.uc2ue.assign(user->uc2ue, user->uc2ue + P0 * Q0);
+    op.ue2uc.assign(user->ue2uc, user->ue2uc + 8 * P0 * Q0);
+    op.dc2de.assign(user->dc2de, user->dc2de + P0 * P0);
+    op.de2dc.assign(user->de2dc, user->de2dc + 8 * P0 * P0);
+    if (user->ue2dc) op.ue2dc.assign(user->ue2dc, user->ue2dc + (size_t)343 * 2 * op.F);
+  }
   Surfaces S;
   make_surfaces(np, &S);
   const int P = S.P, Q = S.Q, F = S.F;
@@ -441,10 +456,9 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d) {
     p->n_ifft = (int)ifn.size();
     KF_TRY(upload(p, &p->fft_nodes, fn));
     KF_TRY(upload(p, &p->ifft_nodes, ifn));
-    std::unordered_map<long long, int> at;
-    at.reserve((size_t)nn * 2);
+    std::vector<std::unordered_map<long long, int>> at(maxd + 1);
     for (int i = 0; i < nn; ++i)
-      at[key_of(d->depth[i], d->path[3 * i], d->path[3 * i + 1], d->path[3 * i + 2])] = i;
+      at[d->depth[i]][key_of(d->path[3 * i], d->path[3 * i + 1], d->path[3 * i + 2])] = i;
     std::vector<int> win, mem;
     for (int pn = 0; pn < nn; ++pn) {
       if (is_leaf(pn)) continue;
@@ -464,8 +478,8 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d) {
                 z = 2 * d->path[3 * pn + 2] - 2 + wz;
             int id = -1;
             if (x >= 0 && y >= 0 && z >= 0 && x < lim && y < lim && z < lim) {
-              auto it = at.find(key_of(cd, x, y, z));
-              if (it != at.end() && has_src(it->second)) id = it->second;
+              auto it = at[cd].find(key_of(x, y, z));
+              if (it != at[cd].end() && has_src(it->second)) id = it->second;
             }
             w[wx + 6 * wy + 36 * wz] = id;
           }
@@ -595,6 +609,12 @@ const char* kfmm_version(void) { return "kifmm_b200 0.1 (sm_100a)"; }
 
 kfmm_status kfmm_plan_create(const kfmm_tree_desc* tree, int np, kfmm_precision precision,
                              kfmm_plan** out) {
+  return kfmm_plan_create_with_operators(tree, np, precision, nullptr, out);
+}
+
+kfmm_status kfmm_plan_create_with_operators(const kfmm_tree_desc* tree, int np,
+                                            kfmm_precision precision,
+                                            const kfmm_operator_set* ops, kfmm_plan** out) {
   if (!out) {
     set_error("kfmm_plan_create: out is NULL");
     return KFMM_ERR_INVALID;
@@ -612,7 +632,7 @@ kfmm_status kfmm_plan_create(const kfmm_tree_desc* tree, int np, kfmm_precision 
   kfmm_plan* p = new kfmm_plan();
   p->np = np;
   p->prec = precision;
-  kfmm_status s = build_plan(p, tree);
+  kfmm_status s = build_plan(p, tree, ops);
   if (s != KFMM_OK) {
     std::string keep = g_error;
     kfmm_plan_destroy(p);
