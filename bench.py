@@ -274,9 +274,11 @@ def main():
     assert np.array_equal(hout.numpy(), pot), "e2e potentials differ from the resident run"
 
     peaks = measured_peaks()
-    fp64_peak = float(os.environ.get("KFMM_FP64_PEAK_TFLOPS", "0") or 0) or None
+    pipes = K.measure_peaks()
+    fp64_peak = pipes["fp64_fma_tflops"]
     achieved = FLOPS_PER_PAIR * st["u_pairs"] / (nf * 1e-3) / 1e12
-    roof = {"bound": "fp64", "kernel": "p2p_fp64_kernel (near field: U+W+X+L2T)",
+    roof = {"bound": "fp64", "peak_source": "kfmm_measure_peak FP64 FMA micro-benchmark, this run",
+            "kernel": "p2p_fp64_kernel (near field: U+W+X+L2T)",
             "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
             "frac": (achieved / fp64_peak) if fp64_peak else None, "traffic": None,
             "algorithmic": f"{FLOPS_PER_PAIR:g} flops/pair x {st['u_pairs']:.4e} pairs per launch",
@@ -311,6 +313,7 @@ def main():
         "clocks": clk,
         "tree": {"nodes": st["num_nodes"], "u_pairs": st["u_pairs"], "v_pairs": st["v_pairs"]},
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
+        "measured_pipes": pipes,
     }
     if rank == 0:
         print(json.dumps(line))

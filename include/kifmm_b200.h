@@ -182,6 +182,12 @@ kfmm_status kfmm_plan_stats(const kfmm_plan* plan, kfmm_stats* stats);
 kfmm_status kfmm_enable_timing(kfmm_plan* plan, int enable);
 kfmm_status kfmm_phase_times(const kfmm_plan* plan, float* ms6);
 
+/* Throughput of the current device's execution pipes, measured by
+ * micro-benchmarks (no reference counterpart; roofline denominators):
+ * what 0: FP64 FMA TFLOP/s, 1: FP32 FMA TFLOP/s, 2: FP32 rsqrt 1e12/s (MUFU),
+ * 3: FP64 rsqrt 1e12/s, 4: FP64 DMMA (mma.sync m8n8k4) TFLOP/s. */
+kfmm_status kfmm_measure_peak(int what, double* value);
+
 const char* kfmm_last_error(void);
 const char* kfmm_version(void);
 

@@ -88,6 +88,7 @@ def lib():
         "kfmm_plan_stats": [vp, ctypes.POINTER(Stats)],
         "kfmm_enable_timing": [vp, i],
         "kfmm_phase_times": [vp, ctypes.POINTER(ctypes.c_float)],
+        "kfmm_measure_peak": [i, _f64p],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -109,6 +110,20 @@ def check(status, what=""):
 
 def _p(a, t=_f64p):
     return a.ctypes.data_as(t)
+
+
+PEAK_KINDS = {"fp64_fma_tflops": 0, "fp32_fma_tflops": 1, "fp32_rsqrt_tops": 2,
+              "fp64_rsqrt_tops": 3, "fp64_dmma_tflops": 4}
+
+
+def measure_peaks():
+    """Micro-benchmarked pipe throughputs of the current device."""
+    out = {}
+    for name, k in PEAK_KINDS.items():
+        v = ctypes.c_double()
+        check(lib().kfmm_measure_peak(k, ctypes.byref(v)), "measure_peak")
+        out[name] = v.value
+    return out
 
 
 def sizes(np_):
