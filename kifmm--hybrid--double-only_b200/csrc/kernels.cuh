@@ -12,6 +12,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace kfmm {
 
 constexpr double kOOFP = 1.0 / (4.0 * 3.14159265358979323846);
@@ -48,9 +50,6 @@ struct P2PParams {
   int P, Q;
 };
 
-constexpr int kP2PThreads = 128;
-constexpr int kP2PStage = 512;
-
 __device__ __forceinline__ double3 surface_point(const double4 c, const double* sp, int k) {
   // centre + radius * unit-surface point, unfused as fmm/trans.cc:92-100
   double3 r;
@@ -60,85 +59,211 @@ __device__ __forceinline__ double3 surface_point(const double4 c, const double* 
   return r;
 }
 
-__global__ void __launch_bounds__(kP2PThreads)
-p2p_fp64_kernel(P2PParams p) {
-  __shared__ double4 stage[kP2PStage];
-  const P2PJob J = p.jobs[blockIdx.x];
-  const int tid = threadIdx.x;
-  const bool active = tid < J.tcnt;
-  const bool warp_active = (tid & ~31) < J.tcnt;
-  double tx = 0, ty = 0, tz = 0;
-  if (active) {
-    if (J.tkind == 0) {
-      double4 t = p.trg4[J.tbeg + tid];
-      tx = t.x;
-      ty = t.y;
-      tz = t.z;
-    } else {
-      double3 s = surface_point(p.ctr[J.tnode], J.tkind == 1 ? p.sp_uc : p.sp_dc, J.tbeg + tid);
-      tx = s.x;
-      ty = s.y;
-      tz = s.z;
+// Mixed precision P2P (kMixed below): coordinates are taken relative to the
+// target set's own node centre in FP64 and then rounded to FP32, so the FP32
+// differences keep ~1e-7 of the box size; 1/r comes from the FP32 reciprocal
+// square root; terms are summed in blocks of 8 whose sums enter a two-sum
+// (hi, lo) pair; the result is formed in FP64 as (hi + lo) / (4 pi).
+__device__ __forceinline__ void two_sum(float& hi, float& lo, float b) {
+  const float s = hi + b;
+  const float bp = s - hi;
+  const float ap = s - bp;
+  lo += (hi - ap) + (b - bp);
+  hi = s;
+}
+
+// ---------------------------------------------------------------------------
+// Warp-autonomous P2P.  One warp owns one job of up to 32*kMaxSlots targets
+// (slot k of lane l is target l + 32k) and walks the job's source sets on its
+// own: no shared memory, no block barriers.  Sources are fetched 32 at a time,
+// one per lane (coalesced), turned into (x, y, z, w) in the lane, and
+// broadcast to the warp with shuffles; each broadcast source meets the lane's
+// `slots` targets, which gives independent dependency chains per source.
+// ---------------------------------------------------------------------------
+constexpr int kWarpJobsPerBlock = 4;
+constexpr int kMaxSlotsFP64 = 2;   // targets per lane, FP64 jobs
+constexpr int kMaxSlotsMixed = 4;  // targets per lane, mixed jobs
+
+template <bool kMixed>
+struct WarpSrc;
+template <>
+struct WarpSrc<false> {
+  double x, y, z, w;
+};
+template <>
+struct WarpSrc<true> {
+  float x, y, z, w;
+};
+
+// Source `idx` of an entry, relative to `org` (mixed) or absolute (FP64).
+template <bool kMixed>
+__device__ __forceinline__ WarpSrc<kMixed> fetch_source(const P2PParams& p, int kind, int node,
+                                                        int base, int idx, const double4 org) {
+  double3 s;
+  double w;
+  if (kind == 0) {
+    const double4 v = p.src4[base + idx];
+    s = make_double3(v.x, v.y, v.z);
+    w = v.w;
+  } else {
+    s = surface_point(p.ctr[node], kind == 1 ? p.sp_ue : p.sp_de, idx);
+    w = (kind == 1 ? p.uden : p.dden)[(size_t)node * p.P + idx];
+  }
+  WarpSrc<kMixed> r;
+  if constexpr (kMixed) {
+    r.x = (float)(s.x - org.x);
+    r.y = (float)(s.y - org.y);
+    r.z = (float)(s.z - org.z);
+    r.w = (float)w;
+  } else {
+    r.x = s.x;
+    r.y = s.y;
+    r.z = s.z;
+    r.w = w;
+  }
+  return r;
+}
+
+template <int NS>
+__device__ __forceinline__ void warp_pairs_fp64(const double (&tx)[NS], const double (&ty)[NS],
+                                                const double (&tz)[NS], double (&acc)[NS],
+                                                const WarpSrc<false>& me, int cnt) {
+#pragma unroll 2
+  for (int k = 0; k < cnt; ++k) {
+    const double sx = __shfl_sync(0xffffffffu, me.x, k);
+    const double sy = __shfl_sync(0xffffffffu, me.y, k);
+    const double sz = __shfl_sync(0xffffffffu, me.z, k);
+    const double sw = __shfl_sync(0xffffffffu, me.w, k);
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+      const double dx = tx[t] - sx, dy = ty[t] - sy, dz = tz[t] - sz;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double inv = rsqrt(r2);
+      acc[t] = fma(sw, r2 > 0.0 ? inv : 0.0, acc[t]);
     }
   }
-  double acc = 0.0;
-  int fill = 0;
-  auto consume = [&](int m) {
-    __syncthreads();
-    if (warp_active) {
-#pragma unroll 4
-      for (int j = 0; j < m; ++j) {
-        const double4 s = stage[j];
-        const double dx = tx - s.x, dy = ty - s.y, dz = tz - s.z;
-        const double r2 = dx * dx + dy * dy + dz * dz;
-        const double inv = rsqrt(r2);
-        acc = fma(s.w, r2 > 0.0 ? inv : 0.0, acc);
+}
+
+template <int NS>
+__device__ __forceinline__ void warp_pairs_mixed(const float (&tx)[NS], const float (&ty)[NS],
+                                                 const float (&tz)[NS], float (&hi)[NS],
+                                                 float (&lo)[NS], const WarpSrc<true>& me,
+                                                 int cnt) {
+  float blk[NS];
+#pragma unroll
+  for (int t = 0; t < NS; ++t) blk[t] = 0.f;
+  int k = 0;
+  for (; k + 8 <= cnt; k += 8) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const float sx = __shfl_sync(0xffffffffu, me.x, k + u);
+      const float sy = __shfl_sync(0xffffffffu, me.y, k + u);
+      const float sz = __shfl_sync(0xffffffffu, me.z, k + u);
+      const float sw = __shfl_sync(0xffffffffu, me.w, k + u);
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+        const float dx = tx[t] - sx, dy = ty[t] - sy, dz = tz[t] - sz;
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        const float inv = rsqrtf(r2);
+        blk[t] = fmaf(sw, r2 > 0.f ? inv : 0.f, blk[t]);
       }
     }
-    __syncthreads();
-  };
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+      two_sum(hi[t], lo[t], blk[t]);
+      blk[t] = 0.f;
+    }
+  }
+  for (; k < cnt; ++k) {
+    const float sx = __shfl_sync(0xffffffffu, me.x, k);
+    const float sy = __shfl_sync(0xffffffffu, me.y, k);
+    const float sz = __shfl_sync(0xffffffffu, me.z, k);
+    const float sw = __shfl_sync(0xffffffffu, me.w, k);
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+      const float dx = tx[t] - sx, dy = ty[t] - sy, dz = tz[t] - sz;
+      const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      blk[t] = fmaf(sw, r2 > 0.f ? rsqrtf(r2) : 0.f, blk[t]);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < NS; ++t) two_sum(hi[t], lo[t], blk[t]);
+}
+
+template <bool kMixed, int NS>
+__device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, int lane) {
+  const double4 org = p.ctr[J.tnode];
+  using T = typename std::conditional<kMixed, float, double>::type;
+  T tx[NS], ty[NS], tz[NS];
+#pragma unroll
+  for (int t = 0; t < NS; ++t) {
+    const int i = lane + 32 * t;
+    double3 q = make_double3(org.x, org.y, org.z);
+    if (i < J.tcnt) {
+      if (J.tkind == 0) {
+        const double4 v = p.trg4[J.tbeg + i];
+        q = make_double3(v.x, v.y, v.z);
+      } else {
+        q = surface_point(org, J.tkind == 1 ? p.sp_uc : p.sp_dc, J.tbeg + i);
+      }
+    }
+    if constexpr (kMixed) {
+      tx[t] = (float)(q.x - org.x);
+      ty[t] = (float)(q.y - org.y);
+      tz[t] = (float)(q.z - org.z);
+    } else {
+      tx[t] = q.x;
+      ty[t] = q.y;
+      tz[t] = q.z;
+    }
+  }
+  double acc[NS];
+  float hi[NS], lo[NS];
+#pragma unroll
+  for (int t = 0; t < NS; ++t) {
+    acc[t] = 0.0;
+    hi[t] = lo[t] = 0.f;
+  }
   for (int e = J.ebeg; e < J.eend; ++e) {
     const int ent = p.entries[e];
     const int kind = ent >> 28, node = ent & 0x0fffffff;
-    int count, base = 0;
-    if (kind == 0) {
-      count = p.src_num[node];
-      base = p.src_beg[node];
-    } else {
-      count = p.P;
-    }
-    int done = 0;
-    while (done < count) {
-      const int m = min(count - done, kP2PStage - fill);
-      for (int k = tid; k < m; k += kP2PThreads) {
-        double4 v;
-        if (kind == 0) {
-          v = p.src4[base + done + k];
-        } else {
-          const double4 c = p.ctr[node];
-          const double3 s = surface_point(c, kind == 1 ? p.sp_ue : p.sp_de, done + k);
-          v.x = s.x;
-          v.y = s.y;
-          v.z = s.z;
-          v.w = (kind == 1 ? p.uden : p.dden)[(size_t)node * p.P + done + k];
-        }
-        stage[fill + k] = v;
-      }
-      fill += m;
-      done += m;
-      if (fill == kP2PStage) {
-        consume(fill);
-        fill = 0;
-      }
+    const int count = kind == 0 ? p.src_num[node] : p.P;
+    const int base = kind == 0 ? p.src_beg[node] : 0;
+    for (int c0 = 0; c0 < count; c0 += 32) {
+      const int cnt = min(32, count - c0);
+      WarpSrc<kMixed> me{};
+      if (lane < cnt) me = fetch_source<kMixed>(p, kind, node, base, c0 + lane, org);
+      if constexpr (kMixed)
+        warp_pairs_mixed<NS>(tx, ty, tz, hi, lo, me, cnt);
+      else
+        warp_pairs_fp64<NS>(tx, ty, tz, acc, me, cnt);
     }
   }
-  if (fill > 0) consume(fill);
-  if (active) {
-    const double r = kOOFP * acc;
-    double* o = p.out + J.out + tid;
-    if (J.mode) *o += r;
-    else *o = r;
+#pragma unroll
+  for (int t = 0; t < NS; ++t) {
+    const int i = lane + 32 * t;
+    if (i < J.tcnt) {
+      const double sum = kMixed ? ((double)hi[t] + (double)lo[t]) : acc[t];
+      const double r = kOOFP * sum;
+      double* o = p.out + J.out + i;
+      if (J.mode) *o += r;
+      else *o = r;
+    }
   }
+}
+
+template <bool kMixed, int kMaxSlots>
+__global__ void __launch_bounds__(32 * kWarpJobsPerBlock, 5)
+p2p_warp_kernel(P2PParams p, int njobs) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * kWarpJobsPerBlock + (threadIdx.x >> 5);
+  if (j >= njobs) return;
+  const P2PJob J = p.jobs[j];
+  const int slots = (J.tcnt + 31) >> 5;
+  if (kMaxSlots >= 4 && slots == 4) warp_job<kMixed, (kMaxSlots >= 4 ? 4 : 1)>(p, J, lane);
+  else if (kMaxSlots >= 3 && slots == 3) warp_job<kMixed, (kMaxSlots >= 3 ? 3 : 1)>(p, J, lane);
+  else if (slots == 2) warp_job<kMixed, 2>(p, J, lane);
+  else warp_job<kMixed, 1>(p, J, lane);
 }
 
 // ---------------------------------------------------------------------------

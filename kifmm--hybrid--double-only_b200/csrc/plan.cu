@@ -381,14 +381,15 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_CUDA(cudaMemset(p->spec, 0, sizeof(double2) * (size_t)nn * F));
   KF_CUDA(cudaMemset(p->effv, 0, sizeof(double2) * (size_t)nn * F));
 
+  const int chunk = 32 * (p->prec == KFMM_MIXED ? kMaxSlotsMixed : kMaxSlotsFP64);
   auto add_chunks = [&](std::vector<P2PJob>& jobs, int tnode, int tkind, int tbeg0, int tcount,
                         int ebeg, int eend, int out0, int mode) {
-    for (int c = 0; c < tcount; c += kP2PThreads) {
+    for (int c = 0; c < tcount; c += chunk) {
       P2PJob j;
       j.tnode = tnode;
       j.tkind = tkind;
       j.tbeg = tbeg0 + c;
-      j.tcnt = std::min(kP2PThreads, tcount - c);
+      j.tcnt = std::min(chunk, tcount - c);
       j.ebeg = ebeg;
       j.eend = eend;
       j.out = out0 + c;
@@ -596,6 +597,17 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
 
 inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
+kfmm_status launch_p2p(const kfmm_plan* p, int njobs, const P2PParams& q, void* stream,
+                       const char* what) {
+  const int blocks = (njobs + kWarpJobsPerBlock - 1) / kWarpJobsPerBlock;
+  if (p->prec == KFMM_MIXED)
+    p2p_warp_kernel<true, kMaxSlotsMixed><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(q, njobs);
+  else
+    p2p_warp_kernel<false, kMaxSlotsFP64><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(q, njobs);
+  KF_CHECK_LAUNCH(std::string("p2p kernel (") + what + ")");
+  return KFMM_OK;
+}
+
 void mark(kfmm_plan* p, int i, cudaStream_t st) {
   if (p->timing) cudaEventRecord(p->ev[i], st);
 }
@@ -709,9 +721,8 @@ kfmm_status kfmm_up_calc(kfmm_plan* p, void* stream) {
     return KFMM_ERR_STATE;
   }
   if (p->n_s2m) {
-    p2p_fp64_kernel<<<p->n_s2m, kP2PThreads, 0, S(stream)>>>(
-        p2p_params(p, p->s2m_jobs, p->s2m_ent, p->chk_up));
-    KF_CHECK_LAUNCH("p2p_fp64_kernel(s2m)");
+    KF_TRY(launch_p2p(p, p->n_s2m, p2p_params(p, p->s2m_jobs, p->s2m_ent, p->chk_up), stream,
+                      "s2m"));
   }
   return launch_gemms(p->up_gemms, 0, p->up_gemms.size(), S(stream));
 }
@@ -746,9 +757,8 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
 kfmm_status kfmm_xlist_calc(kfmm_plan* p, void* stream) {
   if (!p) return KFMM_ERR_INVALID;
   if (p->n_s2l) {
-    p2p_fp64_kernel<<<p->n_s2l, kP2PThreads, 0, S(stream)>>>(
-        p2p_params(p, p->s2l_jobs, p->s2l_ent, p->dchk));
-    KF_CHECK_LAUNCH("p2p_fp64_kernel(s2l)");
+    KF_TRY(launch_p2p(p, p->n_s2l, p2p_params(p, p->s2l_jobs, p->s2l_ent, p->dchk), stream,
+                      "s2l"));
   }
   return KFMM_OK;
 }
@@ -764,9 +774,8 @@ kfmm_status kfmm_ulist_calc(kfmm_plan* p, void* stream) {
     return KFMM_ERR_STATE;
   }
   if (p->n_nf) {
-    p2p_fp64_kernel<<<p->n_nf, kP2PThreads, 0, S(stream)>>>(
-        p2p_params(p, p->nf_jobs, p->nf_ent, p->pot_leaf));
-    KF_CHECK_LAUNCH("p2p_fp64_kernel(near field)");
+    KF_TRY(launch_p2p(p, p->n_nf, p2p_params(p, p->nf_jobs, p->nf_ent, p->pot_leaf), stream,
+                      "near field"));
   }
   return KFMM_OK;
 }

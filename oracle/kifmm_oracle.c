@@ -49,13 +49,21 @@ static double radius(const oracle_tree* t, int node) {
   return 1.0 / (double)(1 << t->depth[node]); /* fmm/input.cc:113-117 */
 }
 
+/* Summation order: 0 = the reference's (ascending), 1 = every sum of the
+ * direct evaluations and matrix-vector products taken in descending order.
+ * Order 1 is an equally valid FP64 evaluation; the spread between the two
+ * measures the algorithm's own rounding floor. */
+static int g_reverse = 0;
+void oracle_set_order(int reverse) { g_reverse = reverse; }
+
 /* ulist__direct_evaluation, fmm/omp.cc:259-283 (SoA targets/sources) */
 static void direct(int nt, const double* tx, const double* ty, const double* tz, double* pot,
                    int ns, const double* sx, const double* sy, const double* sz,
                    const double* w) {
   for (int i = 0; i < nt; i++) {
     double td = 0.0;
-    for (int j = 0; j < ns; j++) {
+    for (int jj = 0; jj < ns; jj++) {
+      int j = g_reverse ? ns - 1 - jj : jj;
       double x = tx[i] - sx[j], y = ty[i] - sy[j], z = tz[i] - sz[j];
       double r = sqrt(x * x + y * y + z * z);
       if (r != 0) td += w[j] / r;
@@ -78,7 +86,8 @@ static void localpos(const oracle_tree* t, int node, const double* sp, int n, do
 
 /* y += A x, A m x n column-major (dgemv, fmm/vecmatop.cc:15-22) */
 static void gemv(int m, int n, const double* A, const double* x, double* y) {
-  for (int j = 0; j < n; j++) {
+  for (int jj = 0; jj < n; jj++) {
+    int j = g_reverse ? n - 1 - jj : jj;
     double xj = x[j];
     const double* a = A + (size_t)j * m;
     for (int i = 0; i < m; i++) y[i] += xj * a[i];

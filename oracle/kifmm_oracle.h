@@ -35,6 +35,11 @@ int oracle_evaluate(const oracle_tree* t, int np, const oracle_ops* ops, const d
                     const double* ty, const double* tz, double* pot, double* uden_out,
                     double* dchk_out, double* dden_out);
 
+/* 0: the reference's summation order; 1: all direct sums and matrix-vector
+ * products in descending order (an equally valid FP64 evaluation, used to
+ * measure the algorithm's own rounding floor).  Process-wide. */
+void oracle_set_order(int reverse);
+
 /* ulist__direct_evaluation over all sources for selected targets (the check of
  * fmm/driver.cc:142-206 with a zeroed accumulator). */
 void oracle_direct(int nt, const double* tx, const double* ty, const double* tz, int ns,

@@ -45,6 +45,8 @@ def lib():
         L.oracle_direct.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p, ctypes.c_int, _f64p,
                                     _f64p, _f64p, _f64p, _f64p]
         L.oracle_direct.restype = None
+        L.oracle_set_order.argtypes = [ctypes.c_int]
+        L.oracle_set_order.restype = None
         _lib = L
     return _lib
 
@@ -77,6 +79,18 @@ def evaluate(tree, np_, ops, pts, want_phases=False):
     if rc != 0:
         raise RuntimeError(f"oracle_evaluate failed: {rc}")
     return (pot, ph) if want_phases else pot
+
+
+def evaluate_reordered(tree, np_, ops, pts):
+    """The oracle with every direct sum and matrix-vector product summed in
+    descending order: the spread to evaluate() is the FP64 rounding floor of
+    the algorithm itself (the pseudo-inverses amplify it by up to their
+    condition number)."""
+    lib().oracle_set_order(1)
+    try:
+        return evaluate(tree, np_, ops, pts)
+    finally:
+        lib().oracle_set_order(0)
 
 
 def direct(tx, ty, tz, sx, sy, sz, den):

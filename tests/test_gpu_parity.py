@@ -4,10 +4,15 @@ build) on the same tree, points and operators, phase by phase and end to end,
 and against the reference CPU build itself where oracle/_ref is present.
 
 Tolerances (plain FP64 path):
-  potentials  : |phi_gpu - phi_oracle| <= 1e-12 * |phi_oracle| per target when
-                densities are non-negative; <= 1e-12 * max|phi_oracle| for the
-                signed-density ellipsoid (per-target relative error is not
-                defined where the potential crosses zero).
+  potentials  : max over targets of |phi_gpu - phi_oracle| / |phi_oracle| (for
+                the signed-density ellipsoid, / max|phi_oracle|: per-target
+                relative error is not defined where the potential crosses
+                zero) <= max(1e-12, 2 * floor), where floor is the same measure
+                between the oracle and the oracle with every sum taken in
+                reverse order.  The floor is the algorithm's own FP64 rounding
+                level: the check-to-equivalent pseudo-inverses amplify any
+                reordering by up to their condition number 0.1^-(np+1); it is
+                below 1e-12 for NP <= 4 and ~6e-11 at NP = 6.
   per-node expansions: max|d| <= 50 eps kappa * max|ref| per node, kappa =
                 0.1^-(np+1) the pseudo-inverse's condition bound: a rounding
                 difference in a check potential reaches the equivalent density
@@ -71,10 +76,13 @@ def test_plain_fp64_vs_oracle(K, oracle_mod, cuda_ok, case):
     e_dc = _node_err(plan.read(1, nn * P), dc, P, trg_nodes)
     e_dd = _node_err(plan.read(2, nn * P), dd, P, trg_nodes)
     e_pot = _pot_err(pot, ref, dist == "ellipsoidSurface")
-    print(f"{_ids(case)}: uden {e_ud:.2e} dchk {e_dc:.2e} dden {e_dd:.2e} pot {e_pot:.2e}")
+    floor = _pot_err(oracle_mod.evaluate_reordered(tarrs, np_, ops, pts), ref,
+                     dist == "ellipsoidSurface")
+    print(f"{_ids(case)}: uden {e_ud:.2e} dchk {e_dc:.2e} dden {e_dd:.2e} pot {e_pot:.2e} "
+          f"(floor {floor:.2e})")
     tol_exp = 50 * 2.2e-16 * 10.0 ** (np_ + 1)
     assert e_ud <= tol_exp and e_dc <= tol_exp and e_dd <= tol_exp
-    assert e_pot <= 1e-12
+    assert e_pot <= max(1e-12, 2 * floor)
 
 
 @pytest.mark.gpu
@@ -101,10 +109,13 @@ def test_plain_fp64_vs_reference_build(K, oracle_mod, cuda_ok, case):
     plan = K.Plan(tree, np_, K.PLAIN_FP64)
     pot_own = plan.evaluate(pts)
     e_own_ops = _pot_err(pot_own, R["pot"], signed)
+    tree_arrays = {k: R[k] for k in oracle_mod.TREE_FIELDS}
+    floor = _pot_err(oracle_mod.evaluate_reordered(tree_arrays, np_, oracle_mod.ops_from_dump(R),
+                                                   pts), R["pot"], signed)
     print(f"{_ids(case)}: vs reference build: {e_same_ops:.2e} (reference operators), "
-          f"{e_own_ops:.2e} (own operators)")
-    assert e_same_ops <= 1e-12
-    assert e_own_ops <= 2e-16 * 10.0 ** (np_ + 1) * 500
+          f"{e_own_ops:.2e} (own operators), floor {floor:.2e}")
+    assert e_same_ops <= max(1e-12, 2 * floor)
+    assert e_own_ops <= max(1e-12, 5 * floor)
     # the reference's own check: rel-L2 against the exact direct sum
     ids = R["check_ids"]
     err = np.linalg.norm(pot[ids] - R["check_direct"]) / np.linalg.norm(pot[ids])
@@ -120,6 +131,7 @@ def test_direct_evaluation_entry(K, oracle_mod, cuda_ok):
     t = rng.uniform(-1, 1, (3, nt))
     s = rng.uniform(-1, 1, (4, ns))
     s[:3, :5] = t[:, :5]  # coincident pairs are skipped
+    s[3] = np.abs(s[3])
     dev = torch.device("cuda:0")
     T = [torch.tensor(v, device=dev) for v in t]
     Sd = [torch.tensor(v, device=dev) for v in s]
@@ -141,3 +153,31 @@ def test_repeat_runs_identical(K, cuda_ok):
     plan.run()
     b = plan.potentials()
     assert np.array_equal(a, b)
+
+
+MIXED_CASES = [("uniform", 65536, 128, 6, 0), ("uniform", 60000, 64, 4, 1),
+               ("ellipsoidSurface", 60000, 40, 4, 0), ("ellipseUniformAngles", 40000, 24, 5, 0)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", MIXED_CASES, ids=_ids)
+def test_mixed_precision_accuracy(K, oracle_mod, cuda_ok, case):
+    """The mixed form (FP32 + compensated sums, FP64 final accumulation) is
+    judged by the reference's own check, the relative L2 error against an
+    exact FP64 direct sum on sampled targets: it must stay within 2x the
+    plain FP64 path's error; its distance to the plain path is reported."""
+    dist, n, ppb, np_, coincide = case
+    pts = K.generate_points(n, dist, coincide, 26, 400)
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], ppb)
+    plain = K.Plan(tree, np_, K.PLAIN_FP64).evaluate(pts)
+    mixed = K.Plan(tree, np_, K.MIXED).evaluate(pts)
+    ids = pts["check_ids"]
+    d = oracle_mod.direct(pts["tx"][ids], pts["ty"][ids], pts["tz"][ids], pts["sx"], pts["sy"],
+                          pts["sz"], pts["den"])
+    e_plain = np.linalg.norm(plain[ids] - d) / np.linalg.norm(d)
+    e_mixed = np.linalg.norm(mixed[ids] - d) / np.linalg.norm(d)
+    vs_plain = np.linalg.norm(mixed - plain) / np.linalg.norm(plain)
+    print(f"{_ids(case)}: rel-L2 vs direct: plain {e_plain:.3e} mixed {e_mixed:.3e}; "
+          f"mixed vs plain {vs_plain:.3e}")
+    assert np.all(np.isfinite(mixed))
+    assert e_mixed <= 2.0 * e_plain
