@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_POINTS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
+                    help="profile one form only (no JSON line)")
     return ap.parse_args()
 
 
@@ -163,10 +165,48 @@ def reference_arm(args):
     print(json.dumps(line))
 
 
+def time_plan(K, plan, sh, stream, steps, warmup, barrier, world, dev):
+    """Device time per kfmm_run (max over ranks), phase breakdown, and the
+    near-field kernel alone (the dominant launch) on its own stream."""
+    import torch
+    for _ in range(warmup):
+        plan.run(sh)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        plan.run(sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    plan.enable_timing(True)
+    plan.run(sh)
+    phases = plan.phase_times()
+    plan.enable_timing(False)
+    nf_ms = []
+    for _ in range(3):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        K.check(K.lib().kfmm_ulist_calc(plan.handle, sh), "ulist")
+        b.record(stream)
+        torch.cuda.synchronize()
+        nf_ms.append(a.elapsed_time(b))
+    return ms, phases, statistics.median(nf_ms)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
+    import ctypes
+
     import torch
     import __graft_entry__
 
@@ -180,60 +220,37 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     n = args.n
 
-    # ---- setup (untimed): points, tree + lists, plan (operators, device arrays)
-    pts = K.generate_points(n, DIST, 0, 26 + rank, 1000)
-    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], PPB)
-    plan = K.Plan(tree, NP, K.PLAIN_FP64)
-    stream = torch.cuda.current_stream(dev)
-    sh = ctypes_stream = stream.cuda_stream
-    plan.set_points(pts, ctypes_stream)
-    st = plan.stats()
-    torch.cuda.synchronize()
-
     def barrier():
         if world > 1:
             torch.distributed.barrier()
 
-    for _ in range(args.warmup):
-        plan.run(sh)
+    # ---- setup (untimed): points, tree + lists, plans (operators, device arrays)
+    pts = K.generate_points(n, DIST, 0, 26 + rank, 1000)
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], PPB)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    plans = {"mixed": K.Plan(tree, NP, K.MIXED), "fp64": K.Plan(tree, NP, K.PLAIN_FP64)}
+    if args.only:
+        pl = plans[args.only]
+        pl.set_points(pts, sh)
+        for _ in range(args.warmup + args.steps):
+            pl.run(sh)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_only": args.only, "n": n}))
+        return
+    for pl in plans.values():
+        pl.set_points(pts, sh)
+    st = plans["fp64"].stats()
     torch.cuda.synchronize()
 
-    # ---- timed: K solves, inputs resident in HBM
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.5)
-    barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        plan.run(sh)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ms = e0.elapsed_time(e1) / args.steps
+    res = {}
+    for name, pl in plans.items():
+        res[name] = time_plan(K, pl, sh, stream, args.steps, args.warmup, barrier, world, dev)
     clk = clocks.stop()
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = n * world / (ms * 1e3)
-
-    # ---- phase breakdown and the dominant kernel timed alone on its stream
-    plan.enable_timing(True)
-    plan.run(sh)
-    phases = plan.phase_times()
-    plan.enable_timing(False)
-    nf_ms = []
-    for _ in range(3):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        K.check(K.lib().kfmm_ulist_calc(plan.handle, sh), "ulist")
-        b.record(stream)
-        torch.cuda.synchronize()
-        nf_ms.append(a.elapsed_time(b))
-    nf = statistics.median(nf_ms)
-    pot = plan.potentials(sh)
+    pots = {name: pl.potentials(sh) for name, pl in plans.items()}
 
     # ---- the reference's check: rel-L2 vs an FP64 direct sum on 1000 targets
     ids = pts["check_ids"]
@@ -245,21 +262,23 @@ def main():
                                            sh), "direct")
     torch.cuda.synchronize()
     direct = direct.cpu().numpy()
-    rel_l2 = float(np.linalg.norm(pot[ids] - direct) / np.linalg.norm(pot[ids]))
+    err = {k: float(np.linalg.norm(v[ids] - direct) / np.linalg.norm(direct))
+           for k, v in pots.items()}
+    mixed_vs_fp64 = float(np.linalg.norm(pots["mixed"] - pots["fp64"]) /
+                          np.linalg.norm(pots["fp64"]))
 
-    # ---- e2e through the C ABI from pinned host buffers
+    # ---- e2e through the C ABI from pinned host buffers (mixed form)
     hp = {k: torch.from_numpy(pts[k]).pin_memory() for k in ("sx", "sy", "sz", "den", "tx", "ty",
                                                            "tz")}
     hout = torch.empty(n, dtype=torch.float64).pin_memory()
-    ptrs = [hp[k].data_ptr() for k in ("sx", "sy", "sz", "den", "tx", "ty", "tz")]
-    import ctypes
     fp = ctypes.POINTER(ctypes.c_double)
-    cargs = [ctypes.cast(p_, fp) for p_ in ptrs] + [ctypes.cast(hout.data_ptr(), fp)]
+    cargs = [ctypes.cast(hp[k].data_ptr(), fp) for k in ("sx", "sy", "sz", "den", "tx", "ty",
+                                                          "tz")] + [ctypes.cast(hout.data_ptr(), fp)]
+    plan = plans["mixed"]
     K.check(K.lib().kfmm_evaluate(plan.handle, *cargs, sh), "evaluate")
     e2e_steps = max(1, min(args.steps, 5))
     barrier()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
     for _ in range(e2e_steps):
@@ -271,53 +290,68 @@ def main():
         t = torch.tensor([e2e_ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    assert np.array_equal(hout.numpy(), pot), "e2e potentials differ from the resident run"
+    assert np.array_equal(hout.numpy(), pots["mixed"]), "e2e potentials differ from the resident run"
 
     peaks = measured_peaks()
     pipes = K.measure_peaks()
-    fp64_peak = pipes["fp64_fma_tflops"]
-    achieved = FLOPS_PER_PAIR * st["u_pairs"] / (nf * 1e-3) / 1e12
-    roof = {"bound": "fp64", "peak_source": "kfmm_measure_peak FP64 FMA micro-benchmark, this run",
-            "kernel": "p2p_fp64_kernel (near field: U+W+X+L2T)",
-            "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-            "frac": (achieved / fp64_peak) if fp64_peak else None, "traffic": None,
-            "algorithmic": f"{FLOPS_PER_PAIR:g} flops/pair x {st['u_pairs']:.4e} pairs per launch",
-            "launch_ms": nf}
+    pairs = st["u_pairs"]
+
+    def roof(name, nf_ms):
+        rate = pairs / (nf_ms * 1e-3)
+        if name == "mixed":
+            ceil = pipes["fp32_rsqrt_tops"] * 1e12
+            bound, kern = "fp32 rsqrt (MUFU)", "p2p_warp_kernel<mixed> (near field: U+W+X+L2T)"
+        else:
+            ceil = pipes["fp64_rsqrt_tops"] * 1e12
+            bound, kern = "fp64 rsqrt", "p2p_warp_kernel<fp64> (near field: U+W+X+L2T)"
+        return {"bound": bound, "kernel": kern,
+                "achieved": FLOPS_PER_PAIR * rate / 1e12, "peak": FLOPS_PER_PAIR * ceil / 1e12,
+                "unit": "TFLOP/s", "frac": rate / ceil, "traffic": None,
+                "algorithmic": f"{FLOPS_PER_PAIR:g} flops/pair (fmm/driver.cc:60) x {pairs:.4e} "
+                               "pairs per launch; peak = one pair per measured reciprocal-sqrt "
+                               "issue",
+                "peak_source": "kfmm_measure_peak micro-benchmark, this run",
+                "pairs_per_s": rate, "launch_ms": nf_ms}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            res = run_reference_cpu(CPU_SAMPLE_N, 1, 0)
-            if res:
-                cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            r = run_reference_cpu(CPU_SAMPLE_N, 1, 0)
+            if r:
+                cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as ex:  # reported, not fatal
             cpu = {"value": None, "error": str(ex)[:200]}
 
-    h2d = 7 * 8 * n
-    d2h = 8 * n
+    ms_mixed, ph_mixed, nf_mixed = res["mixed"]
+    ms_fp64, ph_fp64, nf_fp64 = res["fp64"]
     line = {
-        "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "metric": METRIC, "value": n * world / (ms_mixed * 1e3), "unit": "Mpts/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 (mixed)", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n_points": n, "np": NP, "pts_per_box": PPB,
-                   "distribution": DIST, "precision": "plain_fp64",
+                   "distribution": DIST, "precision": "mixed",
                    "parallelism": f"replicas x{world}" if world > 1 else "single",
                    "l2": "inputs larger than L2 (points 268 MB; expansions and spectra >1 GB)"},
-        "rel_l2_err": rel_l2,
-        "phases_ms": phases,
-        "roofline": roof,
+        "rel_l2_err": err["mixed"], "rel_l2_vs_fp64": mixed_vs_fp64,
+        "fp64": {"value": n * world / (ms_fp64 * 1e3), "unit": "Mpts/s", "ms_per_step": ms_fp64,
+                 "rel_l2_err": err["fp64"], "phases_ms": ph_fp64, "roofline": roof("fp64", nf_fp64)},
+        "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "phases_ms": ph_mixed,
+        "roofline": roof("mixed", nf_mixed),
         "cpu_baseline": cpu,
         "e2e": {"value": n * world / (e2e_ms * 1e3), "unit": "Mpts/s", "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "h2d_bytes_per_step": 7 * 8 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": int(st["launches"]) * args.steps,
         "clocks": clk,
-        "tree": {"nodes": st["num_nodes"], "u_pairs": st["u_pairs"], "v_pairs": st["v_pairs"]},
+        "tree": {"nodes": st["num_nodes"], "u_pairs": pairs, "v_pairs": st["v_pairs"]},
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
         "measured_pipes": pipes,
     }
     if rank == 0:
         print(json.dumps(line))
-    plan.close()
+    for pl in plans.values():
+        pl.close()
     tree.close()
     if world > 1:
         torch.distributed.destroy_process_group()
