@@ -6,7 +6,8 @@
 //   ctr[n]       node centre and radius (cx, cy, cz, r)       double4
 //   uden/dchk/dden[n*P + k]   upward equivalent density, downward check
 //                potential, downward equivalent density      double
-//   spec/effv[n*F + f]        source / target spectra         double2
+//   spec/effv[fb][n][16]      source / target spectra, frequency-blocked
+//                (see spec_index)                            double2
 #pragma once
 
 #include <cuda_runtime.h>
@@ -363,8 +364,16 @@ __global__ void __launch_bounds__(128) gemm_fp64_dmma_kernel(GemmArgs g) {
 // Spectrum index (kz * n + ky) * (np + 1) + kx (r2c halves x).
 // Both transforms are pruned to the np^3 block that holds the surface.
 // ---------------------------------------------------------------------------
+// Spectra are stored frequency-blocked: spec[(fb * nn + node) * kFB + f % kFB]
+// with fb = f / kFB, so one block of frequencies for every box (nn * 256 B)
+// is contiguous and stays resident in L2 while the Hadamard kernel works on it.
+constexpr int kFB = 16;
+__host__ __device__ __forceinline__ size_t spec_index(int f, int node, int nn) {
+  return ((size_t)(f / kFB) * nn + node) * kFB + (f % kFB);
+}
+
 struct FFTParams {
-  int np, P, F;
+  int np, P, F, nn;
   const int* nodes;   // nodes to transform
   const int* depth;
   const int* surf_idx;  // np^3 -> surface index or -1, index (i*np + j)*np + k
@@ -426,7 +435,6 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_fp64_kernel(FFTParams p) 
   }
   __syncthreads();
   // z pass -> spectrum
-  double2* out = p.specout + (size_t)node * p.F;
   for (int q = tid; q < n * n * nk; q += kFFTThreads) {
     const int kx = q % nk, ky = (q / nk) % n, kz = q / (nk * n);
     double ar = 0, ai = 0;
@@ -436,7 +444,7 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_fp64_kernel(FFTParams p) 
       ar += v.x * cs[m] + v.y * sn[m];
       ai += v.y * cs[m] - v.x * sn[m];
     }
-    out[q] = make_double2(ar, ai);
+    p.specout[spec_index(q, node, p.nn)] = make_double2(ar, ai);
   }
 }
 
@@ -455,8 +463,7 @@ __global__ void __launch_bounds__(kFFTThreads) ifft_trg_fp64_kernel(FFTParams p)
     cs[tid] = p.cs[tid];
     sn[tid] = p.sn[tid];
   }
-  const double2* in = p.specin + (size_t)node * p.F;
-  for (int q = tid; q < p.F; q += kFFTThreads) E[q] = in[q];
+  for (int q = tid; q < p.F; q += kFFTThreads) E[q] = p.specin[spec_index(q, node, p.nn)];
   __syncthreads();
   // z inverse, only z in the surface block
   for (int q = tid; q < np * n * nk; q += kFFTThreads) {
@@ -507,48 +514,92 @@ __global__ void __launch_bounds__(kFFTThreads) ifft_trg_fp64_kernel(FFTParams p)
 // (cx,cy,cz) selects translation spectrum (dx+3) + 7 (dy+3) + 49 (dz+3)
 // (fmm/omp_sse_block.cc:581-593).
 struct HadamardParams {
-  int F;
-  const int* win;     // ngroups x 216 node ids (-1 = absent)
-  const int* members; // ngroups x 8 node ids (-1 = no V list)
-  const double2* trans;  // 343 x F
-  const double2* spec;   // node x F
-  double2* effv;         // node x F
+  int nn, ngroups, groups_per_block;
+  const int* win;        // ngroups x 216 node ids (-1 = absent)
+  const int* members;    // ngroups x 8 node ids (-1 = no V list)
+  const double2* trans;  // 343 x Fpad, zero for |delta|_inf <= 1 and f >= F
+  int Fpad;
+  const double2* spec;   // blocked layout
+  double2* effv;         // blocked layout
 };
 
-constexpr int kHadThreads = 128;
+constexpr int kHadThreads = 128;   // 8 groups in flight x 16 frequencies
+constexpr int kHadGroupsInFlight = kHadThreads / kFB;
+constexpr int kHadGroupsPerBlock = 32;
+constexpr size_t kHadSmem = sizeof(double2) * 343 * kFB;  // translation tile
 
+__device__ __forceinline__ void cmac(double& ar, double& ai, const double2 t, const double2 s) {
+  ar = fma(t.x, s.x, ar);
+  ar = fma(-t.y, s.y, ar);
+  ai = fma(t.x, s.y, ai);
+  ai = fma(t.y, s.x, ai);
+}
+
+// One block: one frequency block (blockIdx.y) for groups_per_block groups.
+// Thread (slot, f) owns all 8 members of its group at frequency f.  The 343
+// translation spectra of the frequency block sit in shared memory (zero at
+// the adjacent offsets, so every window entry is a plain multiply-add).  The
+// window is walked row by row in x: a row of 6 source spectra meets, for
+// each of the 4 (cy, cz) member pairs, one row of 7 translation spectra,
+// giving 12 multiply-adds per 7 shared loads.
 __global__ void __launch_bounds__(kHadThreads) hadamard_fp64_kernel(HadamardParams p) {
-  __shared__ int win[216];
-  __shared__ int mem[8];
-  const int g = blockIdx.x;
-  for (int w = threadIdx.x; w < 216; w += kHadThreads) win[w] = p.win[(size_t)g * 216 + w];
-  if (threadIdx.x < 8) mem[threadIdx.x] = p.members[(size_t)g * 8 + threadIdx.x];
-  __syncthreads();
-  const int f = blockIdx.y * kHadThreads + threadIdx.x;
-  if (f >= p.F) return;
-  double ar[8], ai[8];
+  extern __shared__ double2 tsm[];  // [343][kFB]
+  __shared__ int win[kHadGroupsInFlight][216];
+  __shared__ int mem[kHadGroupsInFlight][8];
+  const int fb = blockIdx.y;
+  const int f = threadIdx.x % kFB, slot = threadIdx.x / kFB;
+  for (int q = threadIdx.x; q < 343 * kFB; q += kHadThreads)
+    tsm[q] = p.trans[(size_t)(q / kFB) * p.Fpad + fb * kFB + (q % kFB)];
+  const int g0 = blockIdx.x * p.groups_per_block;
+  const int g1 = min(p.ngroups, g0 + p.groups_per_block);
+  for (int gb = g0; gb < g1; gb += kHadGroupsInFlight) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < kHadGroupsInFlight * 216; q += kHadThreads) {
+      const int g = gb + q / 216;
+      win[q / 216][q % 216] = g < g1 ? p.win[(size_t)g * 216 + q % 216] : -1;
+    }
+    if (threadIdx.x < kHadGroupsInFlight * 8) {
+      const int g = gb + threadIdx.x / 8;
+      mem[threadIdx.x / 8][threadIdx.x % 8] = g < g1 ? p.members[(size_t)g * 8 + threadIdx.x % 8] : -1;
+    }
+    __syncthreads();
+    const int* w = win[slot];
+    double ar[8], ai[8];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) ar[c] = ai[c] = 0.0;
-  for (int w = 0; w < 216; ++w) {
-    const int s = win[w];
-    if (s < 0) continue;
-    const double2 S = p.spec[(size_t)s * p.F + f];
-    const int wx = w % 6, wy = (w / 6) % 6, wz = w / 36;
+    for (int c = 0; c < 8; ++c) ar[c] = ai[c] = 0.0;
+    for (int row = 0; row < 36; ++row) {
+      const int wy = row % 6, wz = row / 6;
+      double2 srow[6];
+#pragma unroll
+      for (int wx = 0; wx < 6; ++wx) {
+        const int s = w[row * 6 + wx];
+        srow[wx] = s >= 0 ? p.spec[((size_t)fb * p.nn + s) * kFB + f] : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int cyz = 0; cyz < 4; ++cyz) {
+        const int cy = cyz >> 1, cz = cyz & 1;
+        const int dy = wy - 2 - cy, dz = wz - 2 - cz;
+        const double2* trow = tsm + ((dz + 3) * 49 + (dy + 3) * 7) * kFB + f;
+        double2 t[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) t[k] = trow[k * kFB];
+#pragma unroll
+        for (int cx = 0; cx < 2; ++cx) {
+          const int c = cx * 4 + cy * 2 + cz;
+#pragma unroll
+          for (int wx = 0; wx < 6; ++wx) {
+            const int k = wx - 2 - cx + 3;  // dx + 3
+            if (k >= 0 && k < 7) cmac(ar[c], ai[c], t[k], srow[wx]);
+          }
+        }
+      }
+    }
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      const int dx = wx - 2 - (c >> 2), dy = wy - 2 - ((c >> 1) & 1), dz = wz - 2 - (c & 1);
-      const int adx = dx < 0 ? -dx : dx, ady = dy < 0 ? -dy : dy, adz = dz < 0 ? -dz : dz;
-      if (max(adx, max(ady, adz)) < 2 || mem[c] < 0) continue;
-      const double2 T = p.trans[(size_t)((dx + 3) + 7 * (dy + 3) + 49 * (dz + 3)) * p.F + f];
-      ar[c] = fma(T.x, S.x, ar[c]);
-      ar[c] = fma(-T.y, S.y, ar[c]);
-      ai[c] = fma(T.x, S.y, ai[c]);
-      ai[c] = fma(T.y, S.x, ai[c]);
+      const int m = mem[slot][c];
+      if (m >= 0) p.effv[((size_t)fb * p.nn + m) * kFB + f] = make_double2(ar[c], ai[c]);
     }
   }
-#pragma unroll
-  for (int c = 0; c < 8; ++c)
-    if (mem[c] >= 0) p.effv[(size_t)mem[c] * p.F + f] = make_double2(ar[c], ai[c]);
 }
 
 // ---------------------------------------------------------------------------

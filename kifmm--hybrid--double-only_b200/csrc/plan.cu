@@ -66,7 +66,7 @@ struct GemmBatch {
 using namespace kfmm;
 
 struct kfmm_plan {
-  int np = 0, P = 0, Q = 0, F = 0, nn = 0, ns = 0, nt = 0, maxdepth = 0;
+  int np = 0, P = 0, Q = 0, F = 0, Fpad = 0, nn = 0, ns = 0, nt = 0, maxdepth = 0;
   kfmm_precision prec = KFMM_PLAIN_FP64;
   std::vector<void*> allocs;
   // tree on device
@@ -196,6 +196,7 @@ FFTParams fft_params(const kfmm_plan* p) {
   f.np = p->np;
   f.P = p->P;
   f.F = p->F;
+  f.nn = p->nn;
   f.depth = p->d_depth;
   f.surf_idx = p->d_surf_idx;
   f.surf_ijk = p->d_surf_ijk;
@@ -325,9 +326,13 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
           st[(size_t)j * 8 * P + c * P + i] = op.de2dc[(size_t)c * P * P + (size_t)j * P + i];
     KF_TRY(upload(p, &p->d_de2dc_stack, st));
   }
+  p->Fpad = (F + kFB - 1) / kFB * kFB;
   {
-    std::vector<double2> tr((size_t)343 * F);
-    for (size_t i = 0; i < tr.size(); ++i) tr[i] = make_double2(op.ue2dc[2 * i], op.ue2dc[2 * i + 1]);
+    std::vector<double2> tr((size_t)343 * p->Fpad, make_double2(0.0, 0.0));
+    for (int id = 0; id < 343; ++id)
+      for (int f = 0; f < F; ++f)
+        tr[(size_t)id * p->Fpad + f] = make_double2(op.ue2dc[2 * ((size_t)id * F + f)],
+                                                    op.ue2dc[2 * ((size_t)id * F + f) + 1]);
     KF_TRY(upload(p, &p->d_trans, tr));
   }
   KF_TRY(upload(p, &p->d_sp_ue, S.ue));
@@ -373,13 +378,13 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_TRY(dalloc(p, &p->uden, (size_t)nn * P));
   KF_TRY(dalloc(p, &p->dchk, (size_t)nn * P));
   KF_TRY(dalloc(p, &p->dden, (size_t)nn * P));
-  KF_TRY(dalloc(p, &p->spec, (size_t)nn * F));
-  KF_TRY(dalloc(p, &p->effv, (size_t)nn * F));
+  KF_TRY(dalloc(p, &p->spec, (size_t)nn * p->Fpad));
+  KF_TRY(dalloc(p, &p->effv, (size_t)nn * p->Fpad));
   KF_CUDA(cudaMemset(p->uden, 0, sizeof(double) * (size_t)nn * P));
   KF_CUDA(cudaMemset(p->dden, 0, sizeof(double) * (size_t)nn * P));
   KF_CUDA(cudaMemset(p->dchk, 0, sizeof(double) * (size_t)nn * P));
-  KF_CUDA(cudaMemset(p->spec, 0, sizeof(double2) * (size_t)nn * F));
-  KF_CUDA(cudaMemset(p->effv, 0, sizeof(double2) * (size_t)nn * F));
+  KF_CUDA(cudaMemset(p->spec, 0, sizeof(double2) * (size_t)nn * p->Fpad));
+  KF_CUDA(cudaMemset(p->effv, 0, sizeof(double2) * (size_t)nn * p->Fpad));
 
   const int chunk = 32 * (p->prec == KFMM_MIXED ? kMaxSlotsMixed : kMaxSlotsFP64);
   auto add_chunks = [&](std::vector<P2PJob>& jobs, int tnode, int tkind, int tbeg0, int tcount,
@@ -581,6 +586,8 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     KF_TRY(upload(p, &p->nf_ent, ent));
   }
 
+  KF_CUDA(cudaFuncSetAttribute(hadamard_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kHadSmem));
   p->ifft_smem = sizeof(double2) * ((size_t)F + (size_t)np * 2 * np * (np + 1));
   KF_CUDA(cudaFuncSetAttribute(ifft_trg_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)p->ifft_smem));
@@ -739,9 +746,10 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
     KF_CHECK_LAUNCH("fft_src_fp64_kernel");
   }
   if (p->n_groups) {
-    HadamardParams h{p->F, p->win, p->members, p->d_trans, p->spec, p->effv};
-    dim3 grid(p->n_groups, (p->F + kHadThreads - 1) / kHadThreads);
-    hadamard_fp64_kernel<<<grid, kHadThreads, 0, S(stream)>>>(h);
+    HadamardParams h{p->nn, p->n_groups, kHadGroupsPerBlock, p->win, p->members, p->d_trans,
+                     p->Fpad, p->spec, p->effv};
+    dim3 grid((p->n_groups + kHadGroupsPerBlock - 1) / kHadGroupsPerBlock, p->Fpad / kFB);
+    hadamard_fp64_kernel<<<grid, kHadThreads, kHadSmem, S(stream)>>>(h);
     KF_CHECK_LAUNCH("hadamard_fp64_kernel");
   }
   if (p->n_ifft) {
@@ -865,7 +873,7 @@ kfmm_status kfmm_read_array(kfmm_plan* p, int which, double* out, size_t count) 
     case 1: src = p->dchk; avail = (size_t)p->nn * p->P; break;
     case 2: src = p->dden; avail = (size_t)p->nn * p->P; break;
     case 3: src = p->pot_leaf; avail = (size_t)p->nt; break;
-    case 4: src = p->spec; avail = (size_t)p->nn * p->F * 2; break;
+    case 4: src = p->spec; avail = (size_t)p->nn * p->Fpad * 2; break;
     default:
       set_error("kfmm_read_array: unknown array");
       return KFMM_ERR_INVALID;
