@@ -76,32 +76,20 @@ __device__ __forceinline__ void two_sum(float& hi, float& lo, float b) {
 // ---------------------------------------------------------------------------
 // Warp-autonomous P2P.  One warp owns one job of up to 32*kMaxSlots targets
 // (slot k of lane l is target l + 32k) and walks the job's source sets on its
-// own: no shared memory, no block barriers.  Sources are fetched 32 at a time,
-// one per lane (coalesced), turned into (x, y, z, w) in the lane, and
-// broadcast to the warp with shuffles; each broadcast source meets the lane's
-// `slots` targets, which gives independent dependency chains per source.
+// own, without block barriers.  Sources are fetched 32 at a time, one per lane
+// (coalesced), prepared in the lane, and written to the warp's own shared
+// buffer; after __syncwarp every lane reads each source back as a broadcast.
+// Each source then meets the lane's `slots` targets: independent dependency
+// chains per source.  r = 0 can only occur between a leaf's own sources and
+// targets (equal coordinates always fall in the same leaf), so only the
+// self entry carries the r > 0 test (fmm/omp.cc:280).
 // ---------------------------------------------------------------------------
 constexpr int kWarpJobsPerBlock = 4;
-constexpr int kMaxSlotsFP64 = 2;   // targets per lane, FP64 jobs
-constexpr int kMaxSlotsMixed = 4;  // targets per lane, mixed jobs
+constexpr int kMaxSlotsFP64 = 4;   // targets per lane, FP64 jobs
+constexpr int kMaxSlotsMixed = 4;  // targets per lane, mixed jobs (even: packed pairs)
 
-template <bool kMixed>
-struct WarpSrc;
-template <>
-struct WarpSrc<false> {
-  double x, y, z, w;
-};
-template <>
-struct WarpSrc<true> {
-  float x, y, z, w;
-};
-
-// Source `idx` of an entry, relative to `org` (mixed) or absolute (FP64).
-template <bool kMixed>
-__device__ __forceinline__ WarpSrc<kMixed> fetch_source(const P2PParams& p, int kind, int node,
-                                                        int base, int idx, const double4 org) {
-  double3 s;
-  double w;
+__device__ __forceinline__ void load_entry_source(const P2PParams& p, int kind, int node,
+                                                  int base, int idx, double3& s, double& w) {
   if (kind == 0) {
     const double4 v = p.src4[base + idx];
     s = make_double3(v.x, v.y, v.z);
@@ -110,142 +98,222 @@ __device__ __forceinline__ WarpSrc<kMixed> fetch_source(const P2PParams& p, int 
     s = surface_point(p.ctr[node], kind == 1 ? p.sp_ue : p.sp_de, idx);
     w = (kind == 1 ? p.uden : p.dden)[(size_t)node * p.P + idx];
   }
-  WarpSrc<kMixed> r;
-  if constexpr (kMixed) {
-    r.x = (float)(s.x - org.x);
-    r.y = (float)(s.y - org.y);
-    r.z = (float)(s.z - org.z);
-    r.w = (float)w;
-  } else {
-    r.x = s.x;
-    r.y = s.y;
-    r.z = s.z;
-    r.w = w;
-  }
-  return r;
 }
 
-template <int NS>
-__device__ __forceinline__ void warp_pairs_fp64(const double (&tx)[NS], const double (&ty)[NS],
-                                                const double (&tz)[NS], double (&acc)[NS],
-                                                const WarpSrc<false>& me, int cnt) {
+template <int NS, bool kGuard>
+__device__ __forceinline__ void pairs_fp64(const double (&tx)[NS], const double (&ty)[NS],
+                                           const double (&tz)[NS], double (&acc)[NS],
+                                           const double4* buf, int cnt) {
 #pragma unroll 2
   for (int k = 0; k < cnt; ++k) {
-    const double sx = __shfl_sync(0xffffffffu, me.x, k);
-    const double sy = __shfl_sync(0xffffffffu, me.y, k);
-    const double sz = __shfl_sync(0xffffffffu, me.z, k);
-    const double sw = __shfl_sync(0xffffffffu, me.w, k);
+    const double4 s = buf[k];
 #pragma unroll
     for (int t = 0; t < NS; ++t) {
-      const double dx = tx[t] - sx, dy = ty[t] - sy, dz = tz[t] - sz;
+      const double dx = tx[t] - s.x, dy = ty[t] - s.y, dz = tz[t] - s.z;
       const double r2 = dx * dx + dy * dy + dz * dz;
-      const double inv = rsqrt(r2);
-      acc[t] = fma(sw, r2 > 0.0 ? inv : 0.0, acc[t]);
+      double inv = rsqrt(r2);
+      if (kGuard) inv = r2 > 0.0 ? inv : 0.0;
+      acc[t] = fma(s.w, inv, acc[t]);
     }
   }
 }
 
-template <int NS>
-__device__ __forceinline__ void warp_pairs_mixed(const float (&tx)[NS], const float (&ty)[NS],
-                                                 const float (&tz)[NS], float (&hi)[NS],
-                                                 float (&lo)[NS], const WarpSrc<true>& me,
-                                                 int cnt) {
-  float blk[NS];
-#pragma unroll
-  for (int t = 0; t < NS; ++t) blk[t] = 0.f;
+// Packed FP32 pairs (sm_100 f32x2 instructions): one instruction updates two
+// targets.  t* hold two targets' coordinates; the source components arrive
+// duplicated in both halves.
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+  return ((unsigned long long)__float_as_uint(hi) << 32) | __float_as_uint(lo);
+}
+__device__ __forceinline__ float lo_of(unsigned long long v) { return __uint_as_float((unsigned)v); }
+__device__ __forceinline__ float hi_of(unsigned long long v) {
+  return __uint_as_float((unsigned)(v >> 32));
+}
+
+template <bool kGuard>
+__device__ __forceinline__ unsigned long long pair_term2(unsigned long long tx,
+                                                         unsigned long long ty,
+                                                         unsigned long long tz, ulonglong2 sxy,
+                                                         ulonglong2 szw, unsigned long long blk) {
+  unsigned long long out;
+  if (kGuard) {
+    asm("{\n"
+        " .reg .b64 dx, dy, dz, r2, inv;\n"
+        " .reg .f32 a, b, ia, ib;\n"
+        " .reg .pred pa, pb;\n"
+        " sub.f32x2 dx, %1, %4;\n"
+        " sub.f32x2 dy, %2, %5;\n"
+        " sub.f32x2 dz, %3, %6;\n"
+        " mul.f32x2 r2, dx, dx;\n"
+        " fma.rn.f32x2 r2, dy, dy, r2;\n"
+        " fma.rn.f32x2 r2, dz, dz, r2;\n"
+        " mov.b64 {a, b}, r2;\n"
+        " rsqrt.approx.ftz.f32 ia, a;\n"
+        " rsqrt.approx.ftz.f32 ib, b;\n"
+        " setp.gt.f32 pa, a, 0f00000000;\n"
+        " setp.gt.f32 pb, b, 0f00000000;\n"
+        " selp.f32 ia, ia, 0f00000000, pa;\n"
+        " selp.f32 ib, ib, 0f00000000, pb;\n"
+        " mov.b64 inv, {ia, ib};\n"
+        " fma.rn.f32x2 %0, %7, inv, %8;\n"
+        "}\n"
+        : "=l"(out)
+        : "l"(tx), "l"(ty), "l"(tz), "l"(sxy.x), "l"(sxy.y), "l"(szw.x), "l"(szw.y), "l"(blk));
+  } else {
+    asm("{\n"
+        " .reg .b64 dx, dy, dz, r2, inv;\n"
+        " .reg .f32 a, b, ia, ib;\n"
+        " sub.f32x2 dx, %1, %4;\n"
+        " sub.f32x2 dy, %2, %5;\n"
+        " sub.f32x2 dz, %3, %6;\n"
+        " mul.f32x2 r2, dx, dx;\n"
+        " fma.rn.f32x2 r2, dy, dy, r2;\n"
+        " fma.rn.f32x2 r2, dz, dz, r2;\n"
+        " mov.b64 {a, b}, r2;\n"
+        " rsqrt.approx.ftz.f32 ia, a;\n"
+        " rsqrt.approx.ftz.f32 ib, b;\n"
+        " mov.b64 inv, {ia, ib};\n"
+        " fma.rn.f32x2 %0, %7, inv, %8;\n"
+        "}\n"
+        : "=l"(out)
+        : "l"(tx), "l"(ty), "l"(tz), "l"(sxy.x), "l"(sxy.y), "l"(szw.x), "l"(szw.y), "l"(blk));
+  }
+  return out;
+}
+
+// buf: per source {x,x},{y,y} then {z,z},{w,w} (two ulonglong2 per source)
+template <int NP2, bool kGuard>
+__device__ __forceinline__ void pairs_mixed(const unsigned long long (&tx)[NP2],
+                                            const unsigned long long (&ty)[NP2],
+                                            const unsigned long long (&tz)[NP2],
+                                            float (&hi)[2 * NP2], float (&lo)[2 * NP2],
+                                            const ulonglong2* buf, int cnt) {
   int k = 0;
-  for (; k + 8 <= cnt; k += 8) {
+  while (k < cnt) {
+    const int m = min(8, cnt - k);
+    unsigned long long blk[NP2];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const float sx = __shfl_sync(0xffffffffu, me.x, k + u);
-      const float sy = __shfl_sync(0xffffffffu, me.y, k + u);
-      const float sz = __shfl_sync(0xffffffffu, me.z, k + u);
-      const float sw = __shfl_sync(0xffffffffu, me.w, k + u);
+    for (int t = 0; t < NP2; ++t) blk[t] = 0ull;
+    if (m == 8) {
 #pragma unroll
-      for (int t = 0; t < NS; ++t) {
-        const float dx = tx[t] - sx, dy = ty[t] - sy, dz = tz[t] - sz;
-        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        const float inv = rsqrtf(r2);
-        blk[t] = fmaf(sw, r2 > 0.f ? inv : 0.f, blk[t]);
+      for (int u = 0; u < 8; ++u) {
+        const ulonglong2 a = buf[2 * (k + u)], b = buf[2 * (k + u) + 1];
+#pragma unroll
+        for (int t = 0; t < NP2; ++t) blk[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a, b, blk[t]);
+      }
+    } else {
+      for (int u = 0; u < m; ++u) {
+        const ulonglong2 a = buf[2 * (k + u)], b = buf[2 * (k + u) + 1];
+#pragma unroll
+        for (int t = 0; t < NP2; ++t) blk[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a, b, blk[t]);
       }
     }
 #pragma unroll
-    for (int t = 0; t < NS; ++t) {
-      two_sum(hi[t], lo[t], blk[t]);
-      blk[t] = 0.f;
+    for (int t = 0; t < NP2; ++t) {
+      two_sum(hi[2 * t], lo[2 * t], lo_of(blk[t]));
+      two_sum(hi[2 * t + 1], lo[2 * t + 1], hi_of(blk[t]));
     }
+    k += m;
   }
-  for (; k < cnt; ++k) {
-    const float sx = __shfl_sync(0xffffffffu, me.x, k);
-    const float sy = __shfl_sync(0xffffffffu, me.y, k);
-    const float sz = __shfl_sync(0xffffffffu, me.z, k);
-    const float sw = __shfl_sync(0xffffffffu, me.w, k);
-#pragma unroll
-    for (int t = 0; t < NS; ++t) {
-      const float dx = tx[t] - sx, dy = ty[t] - sy, dz = tz[t] - sz;
-      const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-      blk[t] = fmaf(sw, r2 > 0.f ? rsqrtf(r2) : 0.f, blk[t]);
-    }
-  }
-#pragma unroll
-  for (int t = 0; t < NS; ++t) two_sum(hi[t], lo[t], blk[t]);
 }
 
 template <bool kMixed, int NS>
-__device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, int lane) {
+__device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, int lane,
+                                         void* wbuf) {
   const double4 org = p.ctr[J.tnode];
-  using T = typename std::conditional<kMixed, float, double>::type;
-  T tx[NS], ty[NS], tz[NS];
+  double q[NS][3];
 #pragma unroll
   for (int t = 0; t < NS; ++t) {
     const int i = lane + 32 * t;
-    double3 q = make_double3(org.x, org.y, org.z);
+    double3 v = make_double3(org.x, org.y, org.z);
     if (i < J.tcnt) {
       if (J.tkind == 0) {
-        const double4 v = p.trg4[J.tbeg + i];
-        q = make_double3(v.x, v.y, v.z);
+        const double4 w = p.trg4[J.tbeg + i];
+        v = make_double3(w.x, w.y, w.z);
       } else {
-        q = surface_point(org, J.tkind == 1 ? p.sp_uc : p.sp_dc, J.tbeg + i);
+        v = surface_point(org, J.tkind == 1 ? p.sp_uc : p.sp_dc, J.tbeg + i);
       }
     }
-    if constexpr (kMixed) {
-      tx[t] = (float)(q.x - org.x);
-      ty[t] = (float)(q.y - org.y);
-      tz[t] = (float)(q.z - org.z);
-    } else {
-      tx[t] = q.x;
-      ty[t] = q.y;
-      tz[t] = q.z;
-    }
+    q[t][0] = v.x;
+    q[t][1] = v.y;
+    q[t][2] = v.z;
   }
-  double acc[NS];
-  float hi[NS], lo[NS];
+  double sum[NS];
+  if constexpr (kMixed) {
+    constexpr int NP2 = NS / 2;
+    unsigned long long tx[NP2], ty[NP2], tz[NP2];
 #pragma unroll
-  for (int t = 0; t < NS; ++t) {
-    acc[t] = 0.0;
-    hi[t] = lo[t] = 0.f;
-  }
-  for (int e = J.ebeg; e < J.eend; ++e) {
-    const int ent = p.entries[e];
-    const int kind = ent >> 28, node = ent & 0x0fffffff;
-    const int count = kind == 0 ? p.src_num[node] : p.P;
-    const int base = kind == 0 ? p.src_beg[node] : 0;
-    for (int c0 = 0; c0 < count; c0 += 32) {
-      const int cnt = min(32, count - c0);
-      WarpSrc<kMixed> me{};
-      if (lane < cnt) me = fetch_source<kMixed>(p, kind, node, base, c0 + lane, org);
-      if constexpr (kMixed)
-        warp_pairs_mixed<NS>(tx, ty, tz, hi, lo, me, cnt);
-      else
-        warp_pairs_fp64<NS>(tx, ty, tz, acc, me, cnt);
+    for (int t = 0; t < NP2; ++t) {
+      tx[t] = pack2((float)(q[2 * t][0] - org.x), (float)(q[2 * t + 1][0] - org.x));
+      ty[t] = pack2((float)(q[2 * t][1] - org.y), (float)(q[2 * t + 1][1] - org.y));
+      tz[t] = pack2((float)(q[2 * t][2] - org.z), (float)(q[2 * t + 1][2] - org.z));
     }
+    float hi[NS], lo[NS];
+#pragma unroll
+    for (int t = 0; t < NS; ++t) hi[t] = lo[t] = 0.f;
+    ulonglong2* buf = (ulonglong2*)wbuf;
+    for (int e = J.ebeg; e < J.eend; ++e) {
+      const int ent = p.entries[e];
+      const int kind = ent >> 28, node = ent & 0x0fffffff;
+      const int count = kind == 0 ? p.src_num[node] : p.P;
+      const int base = kind == 0 ? p.src_beg[node] : 0;
+      const bool guard = kind == 0 && J.tkind == 0 && node == J.tnode;
+      for (int c0 = 0; c0 < count; c0 += 32) {
+        const int cnt = min(32, count - c0);
+        if (lane < cnt) {
+          double3 s;
+          double w;
+          load_entry_source(p, kind, node, base, c0 + lane, s, w);
+          const float fx = (float)(s.x - org.x), fy = (float)(s.y - org.y),
+                      fz = (float)(s.z - org.z), fw = (float)w;
+          buf[2 * lane] = make_ulonglong2(pack2(fx, fx), pack2(fy, fy));
+          buf[2 * lane + 1] = make_ulonglong2(pack2(fz, fz), pack2(fw, fw));
+        }
+        __syncwarp();
+        if (guard) pairs_mixed<NP2, true>(tx, ty, tz, hi, lo, buf, cnt);
+        else pairs_mixed<NP2, false>(tx, ty, tz, hi, lo, buf, cnt);
+        __syncwarp();
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < NS; ++t) sum[t] = (double)hi[t] + (double)lo[t];
+  } else {
+    double tx[NS], ty[NS], tz[NS], acc[NS];
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+      tx[t] = q[t][0];
+      ty[t] = q[t][1];
+      tz[t] = q[t][2];
+      acc[t] = 0.0;
+    }
+    double4* buf = (double4*)wbuf;
+    for (int e = J.ebeg; e < J.eend; ++e) {
+      const int ent = p.entries[e];
+      const int kind = ent >> 28, node = ent & 0x0fffffff;
+      const int count = kind == 0 ? p.src_num[node] : p.P;
+      const int base = kind == 0 ? p.src_beg[node] : 0;
+      const bool guard = kind == 0 && J.tkind == 0 && node == J.tnode;
+      for (int c0 = 0; c0 < count; c0 += 32) {
+        const int cnt = min(32, count - c0);
+        if (lane < cnt) {
+          double3 s;
+          double w;
+          load_entry_source(p, kind, node, base, c0 + lane, s, w);
+          buf[lane] = make_double4(s.x, s.y, s.z, w);
+        }
+        __syncwarp();
+        if (guard) pairs_fp64<NS, true>(tx, ty, tz, acc, buf, cnt);
+        else pairs_fp64<NS, false>(tx, ty, tz, acc, buf, cnt);
+        __syncwarp();
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < NS; ++t) sum[t] = acc[t];
   }
 #pragma unroll
   for (int t = 0; t < NS; ++t) {
     const int i = lane + 32 * t;
     if (i < J.tcnt) {
-      const double sum = kMixed ? ((double)hi[t] + (double)lo[t]) : acc[t];
-      const double r = kOOFP * sum;
+      const double r = kOOFP * sum[t];
       double* o = p.out + J.out + i;
       if (J.mode) *o += r;
       else *o = r;
@@ -254,17 +322,24 @@ __device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, in
 }
 
 template <bool kMixed, int kMaxSlots>
-__global__ void __launch_bounds__(32 * kWarpJobsPerBlock, 5)
+__global__ void __launch_bounds__(32 * kWarpJobsPerBlock, 4)
 p2p_warp_kernel(P2PParams p, int njobs) {
-  const int lane = threadIdx.x & 31;
-  const int j = blockIdx.x * kWarpJobsPerBlock + (threadIdx.x >> 5);
+  __shared__ __align__(16) unsigned char smem[kWarpJobsPerBlock][32 * 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int j = blockIdx.x * kWarpJobsPerBlock + wid;
   if (j >= njobs) return;
   const P2PJob J = p.jobs[j];
   const int slots = (J.tcnt + 31) >> 5;
-  if (kMaxSlots >= 4 && slots == 4) warp_job<kMixed, (kMaxSlots >= 4 ? 4 : 1)>(p, J, lane);
-  else if (kMaxSlots >= 3 && slots == 3) warp_job<kMixed, (kMaxSlots >= 3 ? 3 : 1)>(p, J, lane);
-  else if (slots == 2) warp_job<kMixed, 2>(p, J, lane);
-  else warp_job<kMixed, 1>(p, J, lane);
+  void* wb = smem[wid];
+  if constexpr (kMixed) {
+    if (slots > 2) warp_job<true, 4>(p, J, lane, wb);
+    else warp_job<true, 2>(p, J, lane, wb);
+  } else {
+    if (slots == 4) warp_job<false, 4>(p, J, lane, wb);
+    else if (slots == 3) warp_job<false, 3>(p, J, lane, wb);
+    else if (slots == 2) warp_job<false, 2>(p, J, lane, wb);
+    else warp_job<false, 1>(p, J, lane, wb);
+  }
 }
 
 // ---------------------------------------------------------------------------

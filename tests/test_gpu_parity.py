@@ -116,11 +116,13 @@ def test_plain_fp64_vs_reference_build(K, oracle_mod, cuda_ok, case):
           f"{e_own_ops:.2e} (own operators), floor {floor:.2e}")
     assert e_same_ops <= max(1e-12, 2 * floor)
     assert e_own_ops <= max(1e-12, 5 * floor)
-    # the reference's own check: rel-L2 against the exact direct sum
+    # the reference's own check, rel-L2 against the exact direct sum: no worse
+    # than the reference's by more than the largest per-target deviation
+    # (triangle inequality)
     ids = R["check_ids"]
     err = np.linalg.norm(pot[ids] - R["check_direct"]) / np.linalg.norm(pot[ids])
     ref_err = np.linalg.norm(R["pot"][ids] - R["check_direct"]) / np.linalg.norm(R["pot"][ids])
-    assert err <= 1.01 * ref_err + 1e-14
+    assert err <= ref_err + 1.01 * e_same_ops + 1e-15
 
 
 @pytest.mark.gpu
