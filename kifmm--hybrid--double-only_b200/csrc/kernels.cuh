@@ -65,6 +65,15 @@ __device__ __forceinline__ double3 surface_point(const double4 c, const double* 
 // differences keep ~1e-7 of the box size; 1/r comes from the FP32 reciprocal
 // square root; terms are summed in blocks of 8 whose sums enter a two-sum
 // (hi, lo) pair; the result is formed in FP64 as (hi + lo) / (4 pi).
+template <class R>
+__device__ __forceinline__ void two_sum_any(R& hi, R& lo, R b) {
+  const R s = hi + b;
+  const R bp = s - hi;
+  const R ap = s - bp;
+  lo += (hi - ap) + (b - bp);
+  hi = s;
+}
+
 __device__ __forceinline__ void two_sum(float& hi, float& lo, float b) {
   const float s = hi + b;
   const float bp = s - hi;
@@ -457,15 +466,16 @@ struct FFTParams {
   const double* sn;     // sin(2 pi m / n)
   const double* pln;    // uden (forward) or dchk target (inverse) base
   double* plnout;
-  const double2* specin;
-  double2* specout;
+  const void* specin;   // double2 (FP64 plans) or float2 (mixed plans)
+  void* specout;
 };
 
 constexpr int kFFTThreads = 128;
 constexpr int kMaxNP = 8;
 
 // uden * 2^depth -> scatter -> r2c (omp.cc:386-428, trans.cc:309-358)
-__global__ void __launch_bounds__(kFFTThreads) fft_src_fp64_kernel(FFTParams p) {
+template <class C>
+__global__ void __launch_bounds__(kFFTThreads) fft_src_kernel(FFTParams p) {
   __shared__ double den[kMaxNP * kMaxNP * kMaxNP];
   __shared__ double2 X[kMaxNP * kMaxNP * (kMaxNP + 1)];
   __shared__ double2 Y[kMaxNP * 2 * kMaxNP * (kMaxNP + 1)];
@@ -519,13 +529,17 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_fp64_kernel(FFTParams p) 
       ar += v.x * cs[m] + v.y * sn[m];
       ai += v.y * cs[m] - v.x * sn[m];
     }
-    p.specout[spec_index(q, node, p.nn)] = make_double2(ar, ai);
+    C v;
+    v.x = ar;
+    v.y = ai;
+    ((C*)p.specout)[spec_index(q, node, p.nn)] = v;
   }
 }
 
 // spectrum -> c2r -> gather at the DC surface, scaled by 1/(2np)^3
 // (omp.cc:482-533, trans.cc:383-418).  Writes plnout[node*P + s].
-__global__ void __launch_bounds__(kFFTThreads) ifft_trg_fp64_kernel(FFTParams p) {
+template <class C>
+__global__ void __launch_bounds__(kFFTThreads) ifft_trg_kernel(FFTParams p) {
   extern __shared__ double2 dyn[];
   __shared__ double2 W[kMaxNP * kMaxNP * (kMaxNP + 1)];
   __shared__ double cs[2 * kMaxNP], sn[2 * kMaxNP];
@@ -538,7 +552,10 @@ __global__ void __launch_bounds__(kFFTThreads) ifft_trg_fp64_kernel(FFTParams p)
     cs[tid] = p.cs[tid];
     sn[tid] = p.sn[tid];
   }
-  for (int q = tid; q < p.F; q += kFFTThreads) E[q] = p.specin[spec_index(q, node, p.nn)];
+  for (int q = tid; q < p.F; q += kFFTThreads) {
+    const C v = ((const C*)p.specin)[spec_index(q, node, p.nn)];
+    E[q] = make_double2(v.x, v.y);
+  }
   __syncthreads();
   // z inverse, only z in the surface block
   for (int q = tid; q < np * n * nk; q += kFFTThreads) {
@@ -590,24 +607,41 @@ __global__ void __launch_bounds__(kFFTThreads) ifft_trg_fp64_kernel(FFTParams p)
 // (fmm/omp_sse_block.cc:581-593).
 struct HadamardParams {
   int nn, ngroups, groups_per_block;
-  const int* win;        // ngroups x 216 node ids (-1 = absent)
-  const int* members;    // ngroups x 8 node ids (-1 = no V list)
-  const double2* trans;  // 343 x Fpad, zero for |delta|_inf <= 1 and f >= F
+  const int* win;      // ngroups x 216 node ids (-1 = absent)
+  const int* members;  // ngroups x 8 node ids (-1 = no V list)
+  const void* trans;   // 343 x Fpad complex (double2 or float2), zero for |delta|_inf <= 1, f >= F
   int Fpad;
-  const double2* spec;   // blocked layout
-  double2* effv;         // blocked layout
+  const void* spec;    // blocked layout, double2 or float2
+  void* effv;          // blocked layout, double2 or float2
 };
 
-constexpr int kHadThreads = 128;   // 8 groups in flight x 16 frequencies
+constexpr int kHadThreads = 256;  // 16 groups in flight x 16 frequencies
 constexpr int kHadGroupsInFlight = kHadThreads / kFB;
 constexpr int kHadGroupsPerBlock = 32;
-constexpr size_t kHadSmem = sizeof(double2) * 343 * kFB;  // translation tile
 
-__device__ __forceinline__ void cmac(double& ar, double& ai, const double2 t, const double2 s) {
-  ar = fma(t.x, s.x, ar);
-  ar = fma(-t.y, s.y, ar);
-  ai = fma(t.x, s.y, ai);
-  ai = fma(t.y, s.x, ai);
+template <class C>
+struct HadTraits;
+template <>
+struct HadTraits<double2> {
+  using R = double;
+};
+template <>
+struct HadTraits<float2> {
+  using R = float;
+};
+
+template <class R>
+__device__ __forceinline__ void cmac(R& ar, R& ai, const R tr, const R ti, const R sr,
+                                     const R si) {
+  ar = fma(tr, sr, ar);
+  ar = fma(-ti, si, ar);
+  ai = fma(tr, si, ai);
+  ai = fma(ti, sr, ai);
+}
+
+template <class C>
+__host__ __device__ constexpr size_t had_smem_bytes() {
+  return sizeof(C) * 343 * kFB;
 }
 
 // One block: one frequency block (blockIdx.y) for groups_per_block groups.
@@ -616,17 +650,28 @@ __device__ __forceinline__ void cmac(double& ar, double& ai, const double2 t, co
 // the adjacent offsets, so every window entry is a plain multiply-add).  The
 // window is walked row by row in x: a row of 6 source spectra meets, for
 // each of the 4 (cy, cz) member pairs, one row of 7 translation spectra,
-// giving 12 multiply-adds per 7 shared loads.
-__global__ void __launch_bounds__(kHadThreads) hadamard_fp64_kernel(HadamardParams p) {
-  extern __shared__ double2 tsm[];  // [343][kFB]
+// giving 12 multiply-adds per 7 shared loads; the next row's source spectra
+// are fetched while the current row is multiplied.  FP32 instances
+// accumulate each member over two rows in plain FP32 and add that partial
+// into a two-sum (hi, lo) pair.
+template <class C>
+__global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p) {
+  using R = typename HadTraits<C>::R;
+  constexpr bool kMixed = sizeof(R) == 4;
+  extern __shared__ __align__(16) unsigned char had_dyn[];
+  C* tsm = (C*)had_dyn;  // [343][kFB]
   __shared__ int win[kHadGroupsInFlight][216];
   __shared__ int mem[kHadGroupsInFlight][8];
+  const C* spec = (const C*)p.spec;
+  const C* trans = (const C*)p.trans;
+  C* effv = (C*)p.effv;
   const int fb = blockIdx.y;
   const int f = threadIdx.x % kFB, slot = threadIdx.x / kFB;
   for (int q = threadIdx.x; q < 343 * kFB; q += kHadThreads)
-    tsm[q] = p.trans[(size_t)(q / kFB) * p.Fpad + fb * kFB + (q % kFB)];
+    tsm[q] = trans[(size_t)(q / kFB) * p.Fpad + fb * kFB + (q % kFB)];
   const int g0 = blockIdx.x * p.groups_per_block;
   const int g1 = min(p.ngroups, g0 + p.groups_per_block);
+  const size_t fbase = (size_t)fb * p.nn;
   for (int gb = g0; gb < g1; gb += kHadGroupsInFlight) {
     __syncthreads();
     for (int q = threadIdx.x; q < kHadGroupsInFlight * 216; q += kHadThreads) {
@@ -635,44 +680,72 @@ __global__ void __launch_bounds__(kHadThreads) hadamard_fp64_kernel(HadamardPara
     }
     if (threadIdx.x < kHadGroupsInFlight * 8) {
       const int g = gb + threadIdx.x / 8;
-      mem[threadIdx.x / 8][threadIdx.x % 8] = g < g1 ? p.members[(size_t)g * 8 + threadIdx.x % 8] : -1;
+      mem[threadIdx.x / 8][threadIdx.x % 8] =
+          g < g1 ? p.members[(size_t)g * 8 + threadIdx.x % 8] : -1;
     }
     __syncthreads();
     const int* w = win[slot];
-    double ar[8], ai[8];
+    R ar[8], ai[8], hr[8], hi_[8], lr[8], li[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) ar[c] = ai[c] = 0.0;
+    for (int c = 0; c < 8; ++c) ar[c] = ai[c] = hr[c] = hi_[c] = lr[c] = li[c] = R(0);
+    C nxt[6];
+#pragma unroll
+    for (int wx = 0; wx < 6; ++wx) {
+      const int sid = w[wx];
+      nxt[wx] = sid >= 0 ? spec[(fbase + sid) * kFB + f] : C{R(0), R(0)};
+    }
     for (int row = 0; row < 36; ++row) {
-      const int wy = row % 6, wz = row / 6;
-      double2 srow[6];
+      C srow[6];
 #pragma unroll
-      for (int wx = 0; wx < 6; ++wx) {
-        const int s = w[row * 6 + wx];
-        srow[wx] = s >= 0 ? p.spec[((size_t)fb * p.nn + s) * kFB + f] : make_double2(0.0, 0.0);
+      for (int wx = 0; wx < 6; ++wx) srow[wx] = nxt[wx];
+      if (row + 1 < 36) {
+#pragma unroll
+        for (int wx = 0; wx < 6; ++wx) {
+          const int sid = w[(row + 1) * 6 + wx];
+          nxt[wx] = sid >= 0 ? spec[(fbase + sid) * kFB + f] : C{R(0), R(0)};
+        }
       }
+      const int wy = row % 6, wz = row / 6;
 #pragma unroll
       for (int cyz = 0; cyz < 4; ++cyz) {
         const int cy = cyz >> 1, cz = cyz & 1;
         const int dy = wy - 2 - cy, dz = wz - 2 - cz;
-        const double2* trow = tsm + ((dz + 3) * 49 + (dy + 3) * 7) * kFB + f;
-        double2 t[7];
+        const C* trow = tsm + ((dz + 3) * 49 + (dy + 3) * 7) * kFB + f;
+        C t[7];
 #pragma unroll
         for (int k = 0; k < 7; ++k) t[k] = trow[k * kFB];
 #pragma unroll
-        for (int cx = 0; cx < 2; ++cx) {
-          const int c = cx * 4 + cy * 2 + cz;
+        for (int wx = 0; wx < 6; ++wx)
 #pragma unroll
-          for (int wx = 0; wx < 6; ++wx) {
-            const int k = wx - 2 - cx + 3;  // dx + 3
-            if (k >= 0 && k < 7) cmac(ar[c], ai[c], t[k], srow[wx]);
+          for (int cx = 0; cx < 2; ++cx) {
+            const int c = cx * 4 + cy * 2 + cz;
+            const int k = wx - cx + 1;  // dx + 3
+            cmac<R>(ar[c], ai[c], t[k].x, t[k].y, srow[wx].x, srow[wx].y);
           }
+      }
+      if (kMixed && (row & 1)) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          two_sum_any(hr[c], lr[c], ar[c]);
+          two_sum_any(hi_[c], li[c], ai[c]);
+          ar[c] = ai[c] = R(0);
         }
       }
     }
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       const int m = mem[slot][c];
-      if (m >= 0) p.effv[((size_t)fb * p.nn + m) * kFB + f] = make_double2(ar[c], ai[c]);
+      if (m >= 0) {
+        C v;
+        if (kMixed) {
+          v.x = hr[c] + lr[c];
+          v.y = hi_[c] + li[c];
+        } else {
+          v.x = ar[c];
+          v.y = ai[c];
+        }
+        effv[(fbase + m) * kFB + f] = v;
+      }
     }
   }
 }

@@ -81,10 +81,11 @@ struct kfmm_plan {
   bool have_src = false, have_trg = false;
   // expansions
   double *uden = nullptr, *dchk = nullptr, *dden = nullptr, *chk_up = nullptr, *chk_m = nullptr;
-  double2 *spec = nullptr, *effv = nullptr;
+  void *spec = nullptr, *effv = nullptr;  // double2 (FP64) or float2 (mixed)
+  size_t cplx = sizeof(double2);
   // operators
   double *d_uc2ue = nullptr, *d_ue2uc = nullptr, *d_dc2de = nullptr, *d_de2dc_stack = nullptr;
-  double2* d_trans = nullptr;
+  void* d_trans = nullptr;
   double *d_sp_ue = nullptr, *d_sp_uc = nullptr, *d_sp_de = nullptr, *d_sp_dc = nullptr;
   double *d_cs = nullptr, *d_sn = nullptr;
   int *d_surf_idx = nullptr, *d_surf_ijk = nullptr;
@@ -327,13 +328,25 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     KF_TRY(upload(p, &p->d_de2dc_stack, st));
   }
   p->Fpad = (F + kFB - 1) / kFB * kFB;
-  {
+  p->cplx = p->prec == KFMM_MIXED ? sizeof(float2) : sizeof(double2);
+  if (p->prec == KFMM_MIXED) {
+    std::vector<float2> tr((size_t)343 * p->Fpad, make_float2(0.f, 0.f));
+    for (int id = 0; id < 343; ++id)
+      for (int f = 0; f < F; ++f)
+        tr[(size_t)id * p->Fpad + f] = make_float2((float)op.ue2dc[2 * ((size_t)id * F + f)],
+                                                   (float)op.ue2dc[2 * ((size_t)id * F + f) + 1]);
+    float2* d = nullptr;
+    KF_TRY(upload(p, &d, tr));
+    p->d_trans = d;
+  } else {
     std::vector<double2> tr((size_t)343 * p->Fpad, make_double2(0.0, 0.0));
     for (int id = 0; id < 343; ++id)
       for (int f = 0; f < F; ++f)
         tr[(size_t)id * p->Fpad + f] = make_double2(op.ue2dc[2 * ((size_t)id * F + f)],
                                                     op.ue2dc[2 * ((size_t)id * F + f) + 1]);
-    KF_TRY(upload(p, &p->d_trans, tr));
+    double2* d = nullptr;
+    KF_TRY(upload(p, &d, tr));
+    p->d_trans = d;
   }
   KF_TRY(upload(p, &p->d_sp_ue, S.ue));
   KF_TRY(upload(p, &p->d_sp_uc, S.uc));
@@ -378,13 +391,18 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_TRY(dalloc(p, &p->uden, (size_t)nn * P));
   KF_TRY(dalloc(p, &p->dchk, (size_t)nn * P));
   KF_TRY(dalloc(p, &p->dden, (size_t)nn * P));
-  KF_TRY(dalloc(p, &p->spec, (size_t)nn * p->Fpad));
-  KF_TRY(dalloc(p, &p->effv, (size_t)nn * p->Fpad));
+  {
+    unsigned char *a = nullptr, *b = nullptr;
+    KF_TRY(dalloc(p, &a, (size_t)nn * p->Fpad * p->cplx));
+    KF_TRY(dalloc(p, &b, (size_t)nn * p->Fpad * p->cplx));
+    p->spec = a;
+    p->effv = b;
+  }
   KF_CUDA(cudaMemset(p->uden, 0, sizeof(double) * (size_t)nn * P));
   KF_CUDA(cudaMemset(p->dden, 0, sizeof(double) * (size_t)nn * P));
   KF_CUDA(cudaMemset(p->dchk, 0, sizeof(double) * (size_t)nn * P));
-  KF_CUDA(cudaMemset(p->spec, 0, sizeof(double2) * (size_t)nn * p->Fpad));
-  KF_CUDA(cudaMemset(p->effv, 0, sizeof(double2) * (size_t)nn * p->Fpad));
+  KF_CUDA(cudaMemset(p->spec, 0, p->cplx * (size_t)nn * p->Fpad));
+  KF_CUDA(cudaMemset(p->effv, 0, p->cplx * (size_t)nn * p->Fpad));
 
   const int chunk = 32 * (p->prec == KFMM_MIXED ? kMaxSlotsMixed : kMaxSlotsFP64);
   auto add_chunks = [&](std::vector<P2PJob>& jobs, int tnode, int tkind, int tbeg0, int tcount,
@@ -586,10 +604,15 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     KF_TRY(upload(p, &p->nf_ent, ent));
   }
 
-  KF_CUDA(cudaFuncSetAttribute(hadamard_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kHadSmem));
+  KF_CUDA(cudaFuncSetAttribute(hadamard_kernel<double2>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)had_smem_bytes<double2>()));
+  KF_CUDA(cudaFuncSetAttribute(hadamard_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)had_smem_bytes<float2>()));
   p->ifft_smem = sizeof(double2) * ((size_t)F + (size_t)np * 2 * np * (np + 1));
-  KF_CUDA(cudaFuncSetAttribute(ifft_trg_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  KF_CUDA(cudaFuncSetAttribute(ifft_trg_kernel<double2>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ifft_smem));
+  KF_CUDA(cudaFuncSetAttribute(ifft_trg_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)p->ifft_smem));
   p->stats.num_nodes = nn;
   p->stats.P = P;
@@ -738,26 +761,32 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
   if (!p) return KFMM_ERR_INVALID;
   KF_CUDA(cudaMemsetAsync(p->dchk, 0, sizeof(double) * (size_t)p->nn * p->P, S(stream)));
   FFTParams f = fft_params(p);
+  const bool mixed = p->prec == KFMM_MIXED;
   if (p->n_fft) {
     f.nodes = p->fft_nodes;
     f.pln = p->uden;
     f.specout = p->spec;
-    fft_src_fp64_kernel<<<p->n_fft, kFFTThreads, 0, S(stream)>>>(f);
-    KF_CHECK_LAUNCH("fft_src_fp64_kernel");
+    if (mixed) fft_src_kernel<float2><<<p->n_fft, kFFTThreads, 0, S(stream)>>>(f);
+    else fft_src_kernel<double2><<<p->n_fft, kFFTThreads, 0, S(stream)>>>(f);
+    KF_CHECK_LAUNCH("fft_src_kernel");
   }
   if (p->n_groups) {
     HadamardParams h{p->nn, p->n_groups, kHadGroupsPerBlock, p->win, p->members, p->d_trans,
                      p->Fpad, p->spec, p->effv};
     dim3 grid((p->n_groups + kHadGroupsPerBlock - 1) / kHadGroupsPerBlock, p->Fpad / kFB);
-    hadamard_fp64_kernel<<<grid, kHadThreads, kHadSmem, S(stream)>>>(h);
-    KF_CHECK_LAUNCH("hadamard_fp64_kernel");
+    if (mixed)
+      hadamard_kernel<float2><<<grid, kHadThreads, had_smem_bytes<float2>(), S(stream)>>>(h);
+    else
+      hadamard_kernel<double2><<<grid, kHadThreads, had_smem_bytes<double2>(), S(stream)>>>(h);
+    KF_CHECK_LAUNCH("hadamard_kernel");
   }
   if (p->n_ifft) {
     f.nodes = p->ifft_nodes;
     f.specin = p->effv;
     f.plnout = p->dchk;
-    ifft_trg_fp64_kernel<<<p->n_ifft, kFFTThreads, p->ifft_smem, S(stream)>>>(f);
-    KF_CHECK_LAUNCH("ifft_trg_fp64_kernel");
+    if (mixed) ifft_trg_kernel<float2><<<p->n_ifft, kFFTThreads, p->ifft_smem, S(stream)>>>(f);
+    else ifft_trg_kernel<double2><<<p->n_ifft, kFFTThreads, p->ifft_smem, S(stream)>>>(f);
+    KF_CHECK_LAUNCH("ifft_trg_kernel");
   }
   return KFMM_OK;
 }
@@ -873,7 +902,14 @@ kfmm_status kfmm_read_array(kfmm_plan* p, int which, double* out, size_t count) 
     case 1: src = p->dchk; avail = (size_t)p->nn * p->P; break;
     case 2: src = p->dden; avail = (size_t)p->nn * p->P; break;
     case 3: src = p->pot_leaf; avail = (size_t)p->nt; break;
-    case 4: src = p->spec; avail = (size_t)p->nn * p->Fpad * 2; break;
+    case 4:
+      if (p->prec == KFMM_MIXED) {
+        set_error("kfmm_read_array: spectra of a mixed plan are FP32");
+        return KFMM_ERR_INVALID;
+      }
+      src = p->spec;
+      avail = (size_t)p->nn * p->Fpad * 2;
+      break;
     default:
       set_error("kfmm_read_array: unknown array");
       return KFMM_ERR_INVALID;
