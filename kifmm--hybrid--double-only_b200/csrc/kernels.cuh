@@ -65,15 +65,6 @@ __device__ __forceinline__ double3 surface_point(const double4 c, const double* 
 // differences keep ~1e-7 of the box size; 1/r comes from the FP32 reciprocal
 // square root; terms are summed in blocks of 8 whose sums enter a two-sum
 // (hi, lo) pair; the result is formed in FP64 as (hi + lo) / (4 pi).
-template <class R>
-__device__ __forceinline__ void two_sum_any(R& hi, R& lo, R b) {
-  const R s = hi + b;
-  const R bp = s - hi;
-  const R ap = s - bp;
-  lo += (hi - ap) + (b - bp);
-  hi = s;
-}
-
 __device__ __forceinline__ void two_sum(float& hi, float& lo, float b) {
   const float s = hi + b;
   const float bp = s - hi;
@@ -451,7 +442,7 @@ __global__ void __launch_bounds__(128) gemm_fp64_dmma_kernel(GemmArgs g) {
 // Spectra are stored frequency-blocked: spec[(fb * nn + node) * kFB + f % kFB]
 // with fb = f / kFB, so one block of frequencies for every box (nn * 256 B)
 // is contiguous and stays resident in L2 while the Hadamard kernel works on it.
-constexpr int kFB = 16;
+constexpr int kFB = 8;
 __host__ __device__ __forceinline__ size_t spec_index(int f, int node, int nn) {
   return ((size_t)(f / kFB) * nn + node) * kFB + (f % kFB);
 }
@@ -609,61 +600,82 @@ struct HadamardParams {
   int nn, ngroups, groups_per_block;
   const int* win;      // ngroups x 216 node ids (-1 = absent)
   const int* members;  // ngroups x 8 node ids (-1 = no V list)
-  const void* trans;   // 343 x Fpad complex (double2 or float2), zero for |delta|_inf <= 1, f >= F
+  // 343 x Fpad translation spectra, zero for |delta|_inf <= 1 and f >= F:
+  // double2 (FP64) or float4 {tr, tr, -ti, ti} (mixed, packed operands)
+  const void* trans;
   int Fpad;
-  const void* spec;    // blocked layout, double2 or float2
-  void* effv;          // blocked layout, double2 or float2
+  const void* spec;  // blocked layout, double2 or float2
+  void* effv;        // blocked layout, double2 or float2
 };
 
-constexpr int kHadThreads = 256;  // 16 groups in flight x 16 frequencies
+constexpr int kHadThreads = 256;  // 32 groups in flight x 8 frequencies
 constexpr int kHadGroupsInFlight = kHadThreads / kFB;
-constexpr int kHadGroupsPerBlock = 32;
+constexpr int kHadGroupsPerBlock = 64;
 
-template <class C>
-struct HadTraits;
-template <>
-struct HadTraits<double2> {
-  using R = double;
-};
-template <>
-struct HadTraits<float2> {
-  using R = float;
-};
-
-template <class R>
-__device__ __forceinline__ void cmac(R& ar, R& ai, const R tr, const R ti, const R sr,
-                                     const R si) {
-  ar = fma(tr, sr, ar);
-  ar = fma(-ti, si, ar);
-  ai = fma(tr, si, ai);
-  ai = fma(ti, sr, ai);
+template <bool kMixed>
+__host__ __device__ constexpr size_t had_smem_bytes() {
+  return (kMixed ? sizeof(float4) : sizeof(double2)) * 343 * kFB;
 }
 
-template <class C>
-__host__ __device__ constexpr size_t had_smem_bytes() {
-  return sizeof(C) * 343 * kFB;
+__device__ __forceinline__ void cmac64(double& ar, double& ai, const double2 t, const double2 s) {
+  ar = fma(t.x, s.x, ar);
+  ar = fma(-t.y, s.y, ar);
+  ai = fma(t.x, s.y, ai);
+  ai = fma(t.y, s.x, ai);
+}
+
+// acc {re, im} += t * s with packed FP32: t = {tr, tr, -ti, ti}, s = {sr, si},
+// sw = {si, sr}.
+__device__ __forceinline__ unsigned long long cmac32x2(unsigned long long acc, const float4 t,
+                                                       unsigned long long s,
+                                                       unsigned long long sw) {
+  const unsigned long long t01 = pack2(t.x, t.y), t23 = pack2(t.z, t.w);
+  asm("fma.rn.f32x2 %0, %1, %2, %0;\n"
+      "fma.rn.f32x2 %0, %3, %4, %0;\n"
+      : "+l"(acc)
+      : "l"(t01), "l"(s), "l"(t23), "l"(sw));
+  return acc;
+}
+
+// packed two-sum: (hi, lo) += b, both halves at once
+__device__ __forceinline__ void two_sum32x2(unsigned long long& hi, unsigned long long& lo,
+                                            unsigned long long b) {
+  asm("{\n"
+      " .reg .b64 s, bp, ap, t1, t2;\n"
+      " add.f32x2 s, %0, %2;\n"
+      " sub.f32x2 bp, s, %0;\n"
+      " sub.f32x2 ap, s, bp;\n"
+      " sub.f32x2 t1, %0, ap;\n"
+      " sub.f32x2 t2, %2, bp;\n"
+      " add.f32x2 %1, %1, t1;\n"
+      " add.f32x2 %1, %1, t2;\n"
+      " mov.b64 %0, s;\n"
+      "}\n"
+      : "+l"(hi), "+l"(lo)
+      : "l"(b));
 }
 
 // One block: one frequency block (blockIdx.y) for groups_per_block groups.
-// Thread (slot, f) owns all 8 members of its group at frequency f.  The 343
-// translation spectra of the frequency block sit in shared memory (zero at
-// the adjacent offsets, so every window entry is a plain multiply-add).  The
-// window is walked row by row in x: a row of 6 source spectra meets, for
-// each of the 4 (cy, cz) member pairs, one row of 7 translation spectra,
-// giving 12 multiply-adds per 7 shared loads; the next row's source spectra
-// are fetched while the current row is multiplied.  FP32 instances
-// accumulate each member over two rows in plain FP32 and add that partial
-// into a two-sum (hi, lo) pair.
-template <class C>
+// Thread (slot, f) owns all 8 members of its group at frequency f; a warp
+// holds 4 groups at the same 8 frequencies, so every translation load is
+// shared by 4 groups.  The 343 translation spectra of the frequency block sit
+// in shared memory (zero at the adjacent offsets: every window entry is a
+// plain multiply-add).  The window is walked row by row in x: a row of 6
+// source spectra meets, for each of the 4 (cy, cz) member pairs, one row of 7
+// translation spectra: 12 complex multiply-adds per 7 shared loads; the next
+// row's source spectra are fetched while the current row is multiplied.
+// The FP32 instance (mixed form) uses packed f32x2 multiply-adds and adds
+// each member's two-row partial sums into a two-sum (hi, lo) pair.
+template <bool kMixed>
 __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p) {
-  using R = typename HadTraits<C>::R;
-  constexpr bool kMixed = sizeof(R) == 4;
   extern __shared__ __align__(16) unsigned char had_dyn[];
-  C* tsm = (C*)had_dyn;  // [343][kFB]
   __shared__ int win[kHadGroupsInFlight][216];
   __shared__ int mem[kHadGroupsInFlight][8];
+  using C = typename std::conditional<kMixed, float2, double2>::type;
+  using TT = typename std::conditional<kMixed, float4, double2>::type;
+  TT* tsm = (TT*)had_dyn;  // [343][kFB]
   const C* spec = (const C*)p.spec;
-  const C* trans = (const C*)p.trans;
+  const TT* trans = (const TT*)p.trans;
   C* effv = (C*)p.effv;
   const int fb = blockIdx.y;
   const int f = threadIdx.x % kFB, slot = threadIdx.x / kFB;
@@ -678,73 +690,103 @@ __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p)
       const int g = gb + q / 216;
       win[q / 216][q % 216] = g < g1 ? p.win[(size_t)g * 216 + q % 216] : -1;
     }
-    if (threadIdx.x < kHadGroupsInFlight * 8) {
-      const int g = gb + threadIdx.x / 8;
-      mem[threadIdx.x / 8][threadIdx.x % 8] =
-          g < g1 ? p.members[(size_t)g * 8 + threadIdx.x % 8] : -1;
+    for (int q = threadIdx.x; q < kHadGroupsInFlight * 8; q += kHadThreads) {
+      const int g = gb + q / 8;
+      mem[q / 8][q % 8] = g < g1 ? p.members[(size_t)g * 8 + q % 8] : -1;
     }
     __syncthreads();
     const int* w = win[slot];
-    R ar[8], ai[8], hr[8], hi_[8], lr[8], li[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) ar[c] = ai[c] = hr[c] = hi_[c] = lr[c] = li[c] = R(0);
     C nxt[6];
 #pragma unroll
     for (int wx = 0; wx < 6; ++wx) {
       const int sid = w[wx];
-      nxt[wx] = sid >= 0 ? spec[(fbase + sid) * kFB + f] : C{R(0), R(0)};
+      nxt[wx] = sid >= 0 ? spec[(fbase + sid) * kFB + f] : C{0, 0};
     }
-    for (int row = 0; row < 36; ++row) {
-      C srow[6];
+    if constexpr (kMixed) {
+      unsigned long long acc[8], hi[8], lo[8];
 #pragma unroll
-      for (int wx = 0; wx < 6; ++wx) srow[wx] = nxt[wx];
-      if (row + 1 < 36) {
+      for (int c = 0; c < 8; ++c) acc[c] = hi[c] = lo[c] = 0ull;
+      for (int row = 0; row < 36; ++row) {
+        unsigned long long sr[6], sw[6];
 #pragma unroll
         for (int wx = 0; wx < 6; ++wx) {
-          const int sid = w[(row + 1) * 6 + wx];
-          nxt[wx] = sid >= 0 ? spec[(fbase + sid) * kFB + f] : C{R(0), R(0)};
+          sr[wx] = pack2(nxt[wx].x, nxt[wx].y);
+          sw[wx] = pack2(nxt[wx].y, nxt[wx].x);
         }
-      }
-      const int wy = row % 6, wz = row / 6;
+        if (row + 1 < 36) {
 #pragma unroll
-      for (int cyz = 0; cyz < 4; ++cyz) {
-        const int cy = cyz >> 1, cz = cyz & 1;
-        const int dy = wy - 2 - cy, dz = wz - 2 - cz;
-        const C* trow = tsm + ((dz + 3) * 49 + (dy + 3) * 7) * kFB + f;
-        C t[7];
-#pragma unroll
-        for (int k = 0; k < 7; ++k) t[k] = trow[k * kFB];
-#pragma unroll
-        for (int wx = 0; wx < 6; ++wx)
-#pragma unroll
-          for (int cx = 0; cx < 2; ++cx) {
-            const int c = cx * 4 + cy * 2 + cz;
-            const int k = wx - cx + 1;  // dx + 3
-            cmac<R>(ar[c], ai[c], t[k].x, t[k].y, srow[wx].x, srow[wx].y);
+          for (int wx = 0; wx < 6; ++wx) {
+            const int sid = w[(row + 1) * 6 + wx];
+            nxt[wx] = sid >= 0 ? spec[(fbase + sid) * kFB + f] : C{0, 0};
           }
-      }
-      if (kMixed && (row & 1)) {
+        }
+        const int wy = row % 6, wz = row / 6;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          two_sum_any(hr[c], lr[c], ar[c]);
-          two_sum_any(hi_[c], li[c], ai[c]);
-          ar[c] = ai[c] = R(0);
+        for (int cyz = 0; cyz < 4; ++cyz) {
+          const int cy = cyz >> 1, cz = cyz & 1;
+          const TT* trow = tsm + ((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * kFB + f;
+          TT t[7];
+#pragma unroll
+          for (int k = 0; k < 7; ++k) t[k] = trow[k * kFB];
+#pragma unroll
+          for (int wx = 0; wx < 6; ++wx)
+#pragma unroll
+            for (int cx = 0; cx < 2; ++cx) {
+              const int c = cx * 4 + cy * 2 + cz;
+              acc[c] = cmac32x2(acc[c], t[wx - cx + 1], sr[wx], sw[wx]);
+            }
+        }
+        if (row & 1) {
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            two_sum32x2(hi[c], lo[c], acc[c]);
+            acc[c] = 0ull;
+          }
         }
       }
-    }
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const int m = mem[slot][c];
-      if (m >= 0) {
-        C v;
-        if (kMixed) {
-          v.x = hr[c] + lr[c];
-          v.y = hi_[c] + li[c];
-        } else {
-          v.x = ar[c];
-          v.y = ai[c];
+      for (int c = 0; c < 8; ++c) {
+        const int m = mem[slot][c];
+        if (m >= 0)
+          effv[(fbase + m) * kFB + f] =
+              make_float2(lo_of(hi[c]) + lo_of(lo[c]), hi_of(hi[c]) + hi_of(lo[c]));
+      }
+    } else {
+      double ar[8], ai[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) ar[c] = ai[c] = 0.0;
+      for (int row = 0; row < 36; ++row) {
+        C srow[6];
+#pragma unroll
+        for (int wx = 0; wx < 6; ++wx) srow[wx] = nxt[wx];
+        if (row + 1 < 36) {
+#pragma unroll
+          for (int wx = 0; wx < 6; ++wx) {
+            const int sid = w[(row + 1) * 6 + wx];
+            nxt[wx] = sid >= 0 ? spec[(fbase + sid) * kFB + f] : C{0, 0};
+          }
         }
-        effv[(fbase + m) * kFB + f] = v;
+        const int wy = row % 6, wz = row / 6;
+#pragma unroll
+        for (int cyz = 0; cyz < 4; ++cyz) {
+          const int cy = cyz >> 1, cz = cyz & 1;
+          const TT* trow = tsm + ((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * kFB + f;
+          TT t[7];
+#pragma unroll
+          for (int k = 0; k < 7; ++k) t[k] = trow[k * kFB];
+#pragma unroll
+          for (int wx = 0; wx < 6; ++wx)
+#pragma unroll
+            for (int cx = 0; cx < 2; ++cx) {
+              const int c = cx * 4 + cy * 2 + cz;
+              cmac64(ar[c], ai[c], t[wx - cx + 1], srow[wx]);
+            }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int m = mem[slot][c];
+        if (m >= 0) effv[(fbase + m) * kFB + f] = make_double2(ar[c], ai[c]);
       }
     }
   }

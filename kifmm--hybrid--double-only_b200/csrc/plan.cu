@@ -330,12 +330,14 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   p->Fpad = (F + kFB - 1) / kFB * kFB;
   p->cplx = p->prec == KFMM_MIXED ? sizeof(float2) : sizeof(double2);
   if (p->prec == KFMM_MIXED) {
-    std::vector<float2> tr((size_t)343 * p->Fpad, make_float2(0.f, 0.f));
+    std::vector<float4> tr((size_t)343 * p->Fpad, make_float4(0.f, 0.f, 0.f, 0.f));
     for (int id = 0; id < 343; ++id)
-      for (int f = 0; f < F; ++f)
-        tr[(size_t)id * p->Fpad + f] = make_float2((float)op.ue2dc[2 * ((size_t)id * F + f)],
-                                                   (float)op.ue2dc[2 * ((size_t)id * F + f) + 1]);
-    float2* d = nullptr;
+      for (int f = 0; f < F; ++f) {
+        const float re = (float)op.ue2dc[2 * ((size_t)id * F + f)];
+        const float im = (float)op.ue2dc[2 * ((size_t)id * F + f) + 1];
+        tr[(size_t)id * p->Fpad + f] = make_float4(re, re, -im, im);
+      }
+    float4* d = nullptr;
     KF_TRY(upload(p, &d, tr));
     p->d_trans = d;
   } else {
@@ -604,11 +606,11 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     KF_TRY(upload(p, &p->nf_ent, ent));
   }
 
-  KF_CUDA(cudaFuncSetAttribute(hadamard_kernel<double2>,
+  KF_CUDA(cudaFuncSetAttribute(hadamard_kernel<false>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)had_smem_bytes<double2>()));
-  KF_CUDA(cudaFuncSetAttribute(hadamard_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)had_smem_bytes<float2>()));
+                               (int)had_smem_bytes<false>()));
+  KF_CUDA(cudaFuncSetAttribute(hadamard_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)had_smem_bytes<true>()));
   p->ifft_smem = sizeof(double2) * ((size_t)F + (size_t)np * 2 * np * (np + 1));
   KF_CUDA(cudaFuncSetAttribute(ifft_trg_kernel<double2>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ifft_smem));
@@ -775,9 +777,9 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
                      p->Fpad, p->spec, p->effv};
     dim3 grid((p->n_groups + kHadGroupsPerBlock - 1) / kHadGroupsPerBlock, p->Fpad / kFB);
     if (mixed)
-      hadamard_kernel<float2><<<grid, kHadThreads, had_smem_bytes<float2>(), S(stream)>>>(h);
+      hadamard_kernel<true><<<grid, kHadThreads, had_smem_bytes<true>(), S(stream)>>>(h);
     else
-      hadamard_kernel<double2><<<grid, kHadThreads, had_smem_bytes<double2>(), S(stream)>>>(h);
+      hadamard_kernel<false><<<grid, kHadThreads, had_smem_bytes<false>(), S(stream)>>>(h);
     KF_CHECK_LAUNCH("hadamard_kernel");
   }
   if (p->n_ifft) {
