@@ -361,8 +361,6 @@ struct GemmArgs {
   int accumulate;
 };
 
-constexpr int kGemmBM = 64, kGemmBN = 32, kGemmBK = 16;
-
 __device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, double b) {
   asm volatile(
       "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -370,60 +368,85 @@ __device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, doubl
       : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(128) gemm_fp64_dmma_kernel(GemmArgs g) {
-  __shared__ double As[kGemmBK][kGemmBM + 4];
+// A block computes rows [m0, m0 + mrows) of C (mrows <= 160, a multiple of 8)
+// for kGemmBN columns.  8 warps = 4 (rows) x 2 (columns); each warp owns 5 x 4
+// m8n8 tiles, i.e. 20 DMMA per 4-deep k step for 9 shared loads.  The next
+// 16-deep slice of A and B is fetched into registers while the current one
+// is multiplied from shared memory.
+constexpr int kGemmRows = 160, kGemmBN = 64, kGemmBK = 16, kGemmThreads = 256;
+constexpr int kGemmAPT = kGemmRows * kGemmBK / kGemmThreads;  // A elements per thread per slice
+constexpr int kGemmBPT = kGemmBN * kGemmBK / kGemmThreads;    // B elements per thread per slice
+
+__global__ void __launch_bounds__(kGemmThreads, 1) gemm_fp64_dmma_kernel(GemmArgs g, int mrows) {
+  __shared__ double As[kGemmBK][kGemmRows + 2];
   __shared__ double Bs[kGemmBN][kGemmBK + 1];
   __shared__ int boff_s[kGemmBN];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
-  const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * kGemmBN;
+  const int m0 = blockIdx.x * mrows, n0 = blockIdx.y * kGemmBN;
+  const int mend = min(g.M, m0 + mrows);
   if (tid < kGemmBN) boff_s[tid] = (n0 + tid < g.ncol) ? g.boff[n0 + tid] : -1;
-  double acc[4][2][2];
+  double acc[5][4][2];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 5; ++i)
 #pragma unroll
-    for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   __syncthreads();
+  double ra[kGemmAPT], rb[kGemmBPT];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int r = 0; r < kGemmAPT; ++r) {
+      const int idx = tid + r * kGemmThreads;
+      const int m = idx % kGemmRows, k = idx / kGemmRows;
+      const int gm = m0 + m, gk = k0 + k;
+      ra[r] = (gm < mend && gk < g.K) ? g.A[(size_t)gk * g.M + gm] : 0.0;
+    }
+#pragma unroll
+    for (int r = 0; r < kGemmBPT; ++r) {
+      const int idx = tid + r * kGemmThreads;
+      const int k = idx % kGemmBK, n = idx / kGemmBK;
+      const int gk = k0 + k, bo = boff_s[n];
+      rb[r] = (bo >= 0 && gk < g.K) ? g.B[(size_t)bo + gk] : 0.0;
+    }
+  };
+  fetch(0);
   for (int k0 = 0; k0 < g.K; k0 += kGemmBK) {
 #pragma unroll
-    for (int r = 0; r < (kGemmBK * kGemmBM) / 128; ++r) {
-      const int idx = tid + r * 128;
-      const int m = idx % kGemmBM, k = idx / kGemmBM;
-      const int gm = m0 + m, gk = k0 + k;
-      As[k][m] = (gm < g.M && gk < g.K) ? g.A[(size_t)gk * g.M + gm] : 0.0;
+    for (int r = 0; r < kGemmAPT; ++r) {
+      const int idx = tid + r * kGemmThreads;
+      As[idx / kGemmRows][idx % kGemmRows] = ra[r];
     }
 #pragma unroll
-    for (int r = 0; r < (kGemmBK * kGemmBN) / 128; ++r) {
-      const int idx = tid + r * 128;
-      const int k = idx % kGemmBK, n = idx / kGemmBK;
-      const int gk = k0 + k;
-      const int bo = boff_s[n];
-      Bs[n][k] = (bo >= 0 && gk < g.K) ? g.B[(size_t)bo + gk] : 0.0;
+    for (int r = 0; r < kGemmBPT; ++r) {
+      const int idx = tid + r * kGemmThreads;
+      Bs[idx / kGemmBK][idx % kGemmBK] = rb[r];
     }
     __syncthreads();
+    if (k0 + kGemmBK < g.K) fetch(k0 + kGemmBK);
 #pragma unroll
     for (int kk = 0; kk < kGemmBK; kk += 4) {
-      double af[4], bf[2];
+      double af[5], bf[4];
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi) af[mi] = As[kk + (lane & 3)][wm * 32 + mi * 8 + (lane >> 2)];
+      for (int mi = 0; mi < 5; ++mi)
+        af[mi] = As[kk + (lane & 3)][wm * 40 + mi * 8 + (lane >> 2)];
 #pragma unroll
-      for (int ni = 0; ni < 2; ++ni) bf[ni] = Bs[wn * 16 + ni * 8 + (lane >> 2)][kk + (lane & 3)];
+      for (int ni = 0; ni < 4; ++ni) bf[ni] = Bs[wn * 32 + ni * 8 + (lane >> 2)][kk + (lane & 3)];
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
+      for (int mi = 0; mi < 5; ++mi)
 #pragma unroll
-        for (int ni = 0; ni < 2; ++ni) dmma_884(acc[mi][ni][0], acc[mi][ni][1], af[mi], bf[ni]);
+        for (int ni = 0; ni < 4; ++ni) dmma_884(acc[mi][ni][0], acc[mi][ni][1], af[mi], bf[ni]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi)
+  for (int mi = 0; mi < 5; ++mi)
 #pragma unroll
-    for (int ni = 0; ni < 2; ++ni)
+    for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int m = m0 + wm * 32 + mi * 8 + (lane >> 2);
-        const int n = n0 + wn * 16 + ni * 8 + (lane & 3) * 2 + h;
-        if (m < g.M && n < g.ncol) {
+        const int m = m0 + wm * 40 + mi * 8 + (lane >> 2);
+        const int n = n0 + wn * 32 + ni * 8 + (lane & 3) * 2 + h;
+        if (m < mend && n < g.ncol) {
           const double a = g.alpha ? g.alpha[n] : g.alpha_const;
           double* c = g.C + (size_t)g.coff[n] + m;
           const double v = a * acc[mi][ni][h];
@@ -449,7 +472,7 @@ __host__ __device__ __forceinline__ size_t spec_index(int f, int node, int nn) {
 
 struct FFTParams {
   int np, P, F, nn;
-  const int* nodes;   // nodes to transform
+  const int* nodes;     // nodes to transform
   const int* depth;
   const int* surf_idx;  // np^3 -> surface index or -1, index (i*np + j)*np + k
   const int* surf_ijk;  // P x 3
@@ -464,125 +487,165 @@ struct FFTParams {
 constexpr int kFFTThreads = 128;
 constexpr int kMaxNP = 8;
 
-// uden * 2^depth -> scatter -> r2c (omp.cc:386-428, trans.cc:309-358)
-template <class C>
-__global__ void __launch_bounds__(kFFTThreads) fft_src_kernel(FFTParams p) {
-  __shared__ double den[kMaxNP * kMaxNP * kMaxNP];
-  __shared__ double2 X[kMaxNP * kMaxNP * (kMaxNP + 1)];
-  __shared__ double2 Y[kMaxNP * 2 * kMaxNP * (kMaxNP + 1)];
-  __shared__ double cs[2 * kMaxNP], sn[2 * kMaxNP];
-  const int np = p.np, n = 2 * np, h = np / 2, nk = np + 1;
+// Pruned 3-D transforms of one box per block, compiled per NP so every loop
+// over the np^3 surface block unrolls and every twiddle index is a constant
+// (the twiddle loads are then warp-wide broadcasts).  Each pass gives one
+// thread one line of the grid: the x pass a (z, y) row, the y pass a (z, kx)
+// column, the z pass a (ky, kx) column, and each thread produces all outputs
+// of its line from the <= np non-zero inputs.
+template <int NP, class C>
+__global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
+  constexpr int N = 2 * NP, H = NP / 2, NK = NP + 1;
+  __shared__ double den[NP * NP * NP];
+  __shared__ double2 X[NP * NP * NK];
+  __shared__ double2 Y[NP * N * NK];
+  __shared__ double cs[N], sn[N];
   const int node = p.nodes[blockIdx.x];
   const double scale = ldexp(1.0, p.depth[node]);
   const int tid = threadIdx.x;
-  if (tid < n) {
+  if (tid < N) {
     cs[tid] = p.cs[tid];
     sn[tid] = p.sn[tid];
   }
-  for (int q = tid; q < np * np * np; q += kFFTThreads) {
-    const int s = p.surf_idx[q];
-    den[q] = s >= 0 ? p.pln[(size_t)node * p.P + s] * scale : 0.0;
+  for (int q = tid; q < NP * NP * NP; q += kFFTThreads) {
+    const int sidx = p.surf_idx[q];
+    den[q] = sidx >= 0 ? p.pln[(size_t)node * p.P + sidx] * scale : 0.0;
   }
   __syncthreads();
-  // x pass: (k=z, j=y) rows, kx outputs, sum over i=x
-  for (int q = tid; q < np * np * nk; q += kFFTThreads) {
-    const int kx = q % nk, j = (q / nk) % np, k = q / (nk * np);
-    double ar = 0, ai = 0;
-    for (int i = 0; i < np; ++i) {
-      const double v = den[(i * np + j) * np + k];
-      const int m = (kx * (i + h)) % n;
-      ar += v * cs[m];
-      ai -= v * sn[m];
+  // x: row (k = z, j = y), outputs kx
+  if (tid < NP * NP) {
+    const int k = tid / NP, j = tid % NP;
+    double v[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) v[i] = den[(i * NP + j) * NP + k];
+#pragma unroll
+    for (int kx = 0; kx < NK; ++kx) {
+      double ar = 0, ai = 0;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        const int m = (kx * (i + H)) % N;
+        ar = fma(v[i], cs[m], ar);
+        ai = fma(-v[i], sn[m], ai);
+      }
+      X[(k * NP + j) * NK + kx] = make_double2(ar, ai);
     }
-    X[(k * np + j) * nk + kx] = make_double2(ar, ai);
   }
   __syncthreads();
-  // y pass
-  for (int q = tid; q < np * n * nk; q += kFFTThreads) {
-    const int kx = q % nk, ky = (q / nk) % n, k = q / (nk * n);
-    double ar = 0, ai = 0;
-    for (int j = 0; j < np; ++j) {
-      const double2 v = X[(k * np + j) * nk + kx];
-      const int m = (ky * (j + h)) % n;
-      ar += v.x * cs[m] + v.y * sn[m];
-      ai += v.y * cs[m] - v.x * sn[m];
+  // y: column (k, kx), outputs ky
+  if (tid < NP * NK) {
+    const int k = tid / NK, kx = tid % NK;
+    double2 v[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) v[j] = X[(k * NP + j) * NK + kx];
+#pragma unroll
+    for (int ky = 0; ky < N; ++ky) {
+      double ar = 0, ai = 0;
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        const int m = (ky * (j + H)) % N;
+        ar = fma(v[j].x, cs[m], fma(v[j].y, sn[m], ar));
+        ai = fma(v[j].y, cs[m], fma(-v[j].x, sn[m], ai));
+      }
+      Y[(k * N + ky) * NK + kx] = make_double2(ar, ai);
     }
-    Y[(k * n + ky) * nk + kx] = make_double2(ar, ai);
   }
   __syncthreads();
-  // z pass -> spectrum
-  for (int q = tid; q < n * n * nk; q += kFFTThreads) {
-    const int kx = q % nk, ky = (q / nk) % n, kz = q / (nk * n);
-    double ar = 0, ai = 0;
-    for (int k = 0; k < np; ++k) {
-      const double2 v = Y[(k * n + ky) * nk + kx];
-      const int m = (kz * (k + h)) % n;
-      ar += v.x * cs[m] + v.y * sn[m];
-      ai += v.y * cs[m] - v.x * sn[m];
+  // z: column (ky, kx), outputs kz -> spectrum
+  C* out = (C*)p.specout;
+  if (tid < N * NK) {
+    const int ky = tid / NK, kx = tid % NK;
+    double2 v[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) v[k] = Y[(k * N + ky) * NK + kx];
+#pragma unroll
+    for (int kz = 0; kz < N; ++kz) {
+      double ar = 0, ai = 0;
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        const int m = (kz * (k + H)) % N;
+        ar = fma(v[k].x, cs[m], fma(v[k].y, sn[m], ar));
+        ai = fma(v[k].y, cs[m], fma(-v[k].x, sn[m], ai));
+      }
+      C o;
+      o.x = ar;
+      o.y = ai;
+      out[spec_index((kz * N + ky) * NK + kx, node, p.nn)] = o;
     }
-    C v;
-    v.x = ar;
-    v.y = ai;
-    ((C*)p.specout)[spec_index(q, node, p.nn)] = v;
   }
 }
 
 // spectrum -> c2r -> gather at the DC surface, scaled by 1/(2np)^3
 // (omp.cc:482-533, trans.cc:383-418).  Writes plnout[node*P + s].
-template <class C>
-__global__ void __launch_bounds__(kFFTThreads) ifft_trg_kernel(FFTParams p) {
-  extern __shared__ double2 dyn[];
-  __shared__ double2 W[kMaxNP * kMaxNP * (kMaxNP + 1)];
-  __shared__ double cs[2 * kMaxNP], sn[2 * kMaxNP];
-  const int np = p.np, n = 2 * np, h = np / 2, nk = np + 1;
+template <int NP, class C>
+__global__ void __launch_bounds__(kFFTThreads) ifft_trg_np_kernel(FFTParams p) {
+  constexpr int N = 2 * NP, H = NP / 2, NK = NP + 1;
+  __shared__ double2 Z[NP * N * NK];
+  __shared__ double2 W[NP * NP * NK];
+  __shared__ double cs[N], sn[N];
   const int node = p.nodes[blockIdx.x];
   const int tid = threadIdx.x;
-  double2* E = dyn;                 // F
-  double2* Z = dyn + p.F;           // np * n * nk
-  if (tid < n) {
+  if (tid < N) {
     cs[tid] = p.cs[tid];
     sn[tid] = p.sn[tid];
   }
-  for (int q = tid; q < p.F; q += kFFTThreads) {
-    const C v = ((const C*)p.specin)[spec_index(q, node, p.nn)];
-    E[q] = make_double2(v.x, v.y);
-  }
   __syncthreads();
-  // z inverse, only z in the surface block
-  for (int q = tid; q < np * n * nk; q += kFFTThreads) {
-    const int kx = q % nk, ky = (q / nk) % n, k = q / (nk * n);
-    double ar = 0, ai = 0;
-    for (int kz = 0; kz < n; ++kz) {
-      const double2 v = E[(kz * n + ky) * nk + kx];
-      const int m = (kz * (k + h)) % n;
-      ar += v.x * cs[m] - v.y * sn[m];
-      ai += v.y * cs[m] + v.x * sn[m];
+  // z inverse: column (ky, kx), outputs z in the surface block; every
+  // spectrum entry is read exactly once, straight from global memory
+  // (consecutive threads, consecutive entries)
+  const C* in = (const C*)p.specin;
+  if (tid < N * NK) {
+    const int ky = tid / NK, kx = tid % NK;
+    double2 acc[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) acc[k] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int kz = 0; kz < N; ++kz) {
+      const C e = in[spec_index((kz * N + ky) * NK + kx, node, p.nn)];
+      const double2 v = make_double2(e.x, e.y);
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        const int m = (kz * (k + H)) % N;
+        acc[k].x = fma(v.x, cs[m], fma(-v.y, sn[m], acc[k].x));
+        acc[k].y = fma(v.y, cs[m], fma(v.x, sn[m], acc[k].y));
+      }
     }
-    Z[(k * n + ky) * nk + kx] = make_double2(ar, ai);
+#pragma unroll
+    for (int k = 0; k < NP; ++k) Z[(k * N + ky) * NK + kx] = acc[k];
   }
   __syncthreads();
-  // y inverse
-  for (int q = tid; q < np * np * nk; q += kFFTThreads) {
-    const int kx = q % nk, j = (q / nk) % np, k = q / (nk * np);
-    double ar = 0, ai = 0;
-    for (int ky = 0; ky < n; ++ky) {
-      const double2 v = Z[(k * n + ky) * nk + kx];
-      const int m = (ky * (j + h)) % n;
-      ar += v.x * cs[m] - v.y * sn[m];
-      ai += v.y * cs[m] + v.x * sn[m];
+  // y inverse: column (k, kx), outputs y in the surface block
+  if (tid < NP * NK) {
+    const int k = tid / NK, kx = tid % NK;
+    double2 acc[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) acc[j] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int ky = 0; ky < N; ++ky) {
+      const double2 v = Z[(k * N + ky) * NK + kx];
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        const int m = (ky * (j + H)) % N;
+        acc[j].x = fma(v.x, cs[m], fma(-v.y, sn[m], acc[j].x));
+        acc[j].y = fma(v.y, cs[m], fma(v.x, sn[m], acc[j].y));
+      }
     }
-    W[(k * np + j) * nk + kx] = make_double2(ar, ai);
+#pragma unroll
+    for (int j = 0; j < NP; ++j) W[(k * NP + j) * NK + kx] = acc[j];
   }
   __syncthreads();
-  // x: Hermitian half -> real, at surface points only
-  const double inv_g = 1.0 / (double)(n * n * n);
-  for (int s = tid; s < p.P; s += kFFTThreads) {
+  // x: Hermitian half -> real, at the surface points only
+  constexpr double inv_g = 1.0 / (double)(N * N * N);
+  constexpr int P = NP * NP * NP - (NP - 2) * (NP - 2) * (NP - 2);
+  for (int s = tid; s < P; s += kFFTThreads) {
     const int i = p.surf_ijk[3 * s], j = p.surf_ijk[3 * s + 1], k = p.surf_ijk[3 * s + 2];
-    const double2* w = &W[(k * np + j) * nk];
-    const int x = i + h;
-    double acc = w[0].x + ((x & 1) ? -w[np].x : w[np].x);
-    for (int kx = 1; kx < np; ++kx) {
-      const int m = (kx * x) % n;
+    const double2* w = &W[(k * NP + j) * NK];
+    const int x = i + H;
+    double acc = w[0].x + ((x & 1) ? -w[NP].x : w[NP].x);
+    int m = 0;
+#pragma unroll
+    for (int kx = 1; kx < NP; ++kx) {
+      m += x;
+      if (m >= N) m -= N;
       acc += 2.0 * (w[kx].x * cs[m] - w[kx].y * sn[m]);
     }
     p.plnout[(size_t)node * p.P + s] = acc * inv_g;

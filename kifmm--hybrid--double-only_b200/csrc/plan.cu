@@ -98,7 +98,6 @@ struct kfmm_plan {
   int n_fft = 0, n_ifft = 0;
   int *win = nullptr, *members = nullptr;
   int n_groups = 0;
-  size_t ifft_smem = 0;
   kfmm_stats stats{};
   bool timing = false;
   cudaEvent_t ev[7] = {};
@@ -164,8 +163,11 @@ kfmm_status launch_gemms(const std::vector<GemmBatch>& gs, size_t first, size_t 
     const GemmBatch& b = gs[i];
     GemmArgs a{b.A, b.M, b.K, b.B, b.boff, b.C, b.coff, b.alpha, b.alpha_const, b.ncol,
                b.accumulate};
-    dim3 grid((b.M + kGemmBM - 1) / kGemmBM, (b.ncol + kGemmBN - 1) / kGemmBN);
-    gemm_fp64_dmma_kernel<<<grid, 128, 0, st>>>(a);
+    // split the M rows into near-equal chunks of <= kGemmRows, multiples of 8
+    const int chunks = (b.M + kGemmRows - 1) / kGemmRows;
+    const int mrows = ((b.M + chunks - 1) / chunks + 7) / 8 * 8;
+    dim3 grid(chunks, (b.ncol + kGemmBN - 1) / kGemmBN);
+    gemm_fp64_dmma_kernel<<<grid, kGemmThreads, 0, st>>>(a, mrows);
     KF_CHECK_LAUNCH("gemm_fp64_dmma_kernel");
   }
   return KFMM_OK;
@@ -611,11 +613,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
                                (int)had_smem_bytes<false>()));
   KF_CUDA(cudaFuncSetAttribute(hadamard_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)had_smem_bytes<true>()));
-  p->ifft_smem = sizeof(double2) * ((size_t)F + (size_t)np * 2 * np * (np + 1));
-  KF_CUDA(cudaFuncSetAttribute(ifft_trg_kernel<double2>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ifft_smem));
-  KF_CUDA(cudaFuncSetAttribute(ifft_trg_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)p->ifft_smem));
+
   p->stats.num_nodes = nn;
   p->stats.P = P;
   p->stats.Q = Q;
@@ -628,6 +626,32 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
 }
 
 inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+
+template <int NP>
+void fft_launch_np(bool mixed, bool forward, int nblocks, const FFTParams& f, cudaStream_t st) {
+  if (forward) {
+    if (mixed) fft_src_np_kernel<NP, float2><<<nblocks, kFFTThreads, 0, st>>>(f);
+    else fft_src_np_kernel<NP, double2><<<nblocks, kFFTThreads, 0, st>>>(f);
+  } else {
+    if (mixed) ifft_trg_np_kernel<NP, float2><<<nblocks, kFFTThreads, 0, st>>>(f);
+    else ifft_trg_np_kernel<NP, double2><<<nblocks, kFFTThreads, 0, st>>>(f);
+  }
+}
+
+kfmm_status launch_fft(int np, bool mixed, bool forward, int nblocks, const FFTParams& f,
+                       void* stream) {
+  switch (np) {
+    case 3: fft_launch_np<3>(mixed, forward, nblocks, f, S(stream)); break;
+    case 4: fft_launch_np<4>(mixed, forward, nblocks, f, S(stream)); break;
+    case 5: fft_launch_np<5>(mixed, forward, nblocks, f, S(stream)); break;
+    case 6: fft_launch_np<6>(mixed, forward, nblocks, f, S(stream)); break;
+    case 7: fft_launch_np<7>(mixed, forward, nblocks, f, S(stream)); break;
+    case 8: fft_launch_np<8>(mixed, forward, nblocks, f, S(stream)); break;
+    default: set_error("launch_fft: NP out of range"); return KFMM_ERR_UNSUPPORTED;
+  }
+  KF_CHECK_LAUNCH(forward ? "fft_src_np_kernel" : "ifft_trg_np_kernel");
+  return KFMM_OK;
+}
 
 kfmm_status launch_p2p(const kfmm_plan* p, int njobs, const P2PParams& q, void* stream,
                        const char* what) {
@@ -768,9 +792,7 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
     f.nodes = p->fft_nodes;
     f.pln = p->uden;
     f.specout = p->spec;
-    if (mixed) fft_src_kernel<float2><<<p->n_fft, kFFTThreads, 0, S(stream)>>>(f);
-    else fft_src_kernel<double2><<<p->n_fft, kFFTThreads, 0, S(stream)>>>(f);
-    KF_CHECK_LAUNCH("fft_src_kernel");
+    KF_TRY(launch_fft(p->np, mixed, true, p->n_fft, f, stream));
   }
   if (p->n_groups) {
     HadamardParams h{p->nn, p->n_groups, kHadGroupsPerBlock, p->win, p->members, p->d_trans,
@@ -786,9 +808,7 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
     f.nodes = p->ifft_nodes;
     f.specin = p->effv;
     f.plnout = p->dchk;
-    if (mixed) ifft_trg_kernel<float2><<<p->n_ifft, kFFTThreads, p->ifft_smem, S(stream)>>>(f);
-    else ifft_trg_kernel<double2><<<p->n_ifft, kFFTThreads, p->ifft_smem, S(stream)>>>(f);
-    KF_CHECK_LAUNCH("ifft_trg_kernel");
+    KF_TRY(launch_fft(p->np, mixed, false, p->n_ifft, f, stream));
   }
   return KFMM_OK;
 }
