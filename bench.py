@@ -229,15 +229,15 @@ def main():
     tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], PPB)
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
-    plans = {"mixed": K.Plan(tree, NP, K.MIXED), "fp64": K.Plan(tree, NP, K.PLAIN_FP64)}
     if args.only:
-        pl = plans[args.only]
+        pl = K.Plan(tree, NP, K.MIXED if args.only == "mixed" else K.PLAIN_FP64)
         pl.set_points(pts, sh)
         for _ in range(args.warmup + args.steps):
             pl.run(sh)
         torch.cuda.synchronize()
         print(json.dumps({"profile_only": args.only, "n": n}))
         return
+    plans = {"mixed": K.Plan(tree, NP, K.MIXED), "fp64": K.Plan(tree, NP, K.PLAIN_FP64)}
     for pl in plans.values():
         pl.set_points(pts, sh)
     st = plans["fp64"].stats()

@@ -513,8 +513,8 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
   }
   __syncthreads();
   // x: row (k = z, j = y), outputs kx
-  if (tid < NP * NP) {
-    const int k = tid / NP, j = tid % NP;
+  for (int t = tid; t < NP * NP; t += kFFTThreads) {
+    const int k = t / NP, j = t % NP;
     double v[NP];
 #pragma unroll
     for (int i = 0; i < NP; ++i) v[i] = den[(i * NP + j) * NP + k];
@@ -532,8 +532,8 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
   }
   __syncthreads();
   // y: column (k, kx), outputs ky
-  if (tid < NP * NK) {
-    const int k = tid / NK, kx = tid % NK;
+  for (int t = tid; t < NP * NK; t += kFFTThreads) {
+    const int k = t / NK, kx = t % NK;
     double2 v[NP];
 #pragma unroll
     for (int j = 0; j < NP; ++j) v[j] = X[(k * NP + j) * NK + kx];
@@ -552,8 +552,8 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
   __syncthreads();
   // z: column (ky, kx), outputs kz -> spectrum
   C* out = (C*)p.specout;
-  if (tid < N * NK) {
-    const int ky = tid / NK, kx = tid % NK;
+  for (int t = tid; t < N * NK; t += kFFTThreads) {
+    const int ky = t / NK, kx = t % NK;
     double2 v[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) v[k] = Y[(k * N + ky) * NK + kx];
@@ -593,8 +593,8 @@ __global__ void __launch_bounds__(kFFTThreads) ifft_trg_np_kernel(FFTParams p) {
   // spectrum entry is read exactly once, straight from global memory
   // (consecutive threads, consecutive entries)
   const C* in = (const C*)p.specin;
-  if (tid < N * NK) {
-    const int ky = tid / NK, kx = tid % NK;
+  for (int t = tid; t < N * NK; t += kFFTThreads) {
+    const int ky = t / NK, kx = t % NK;
     double2 acc[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) acc[k] = make_double2(0.0, 0.0);
@@ -614,8 +614,8 @@ __global__ void __launch_bounds__(kFFTThreads) ifft_trg_np_kernel(FFTParams p) {
   }
   __syncthreads();
   // y inverse: column (k, kx), outputs y in the surface block
-  if (tid < NP * NK) {
-    const int k = tid / NK, kx = tid % NK;
+  for (int t = tid; t < NP * NK; t += kFFTThreads) {
+    const int k = t / NK, kx = t % NK;
     double2 acc[NP];
 #pragma unroll
     for (int j = 0; j < NP; ++j) acc[j] = make_double2(0.0, 0.0);
