@@ -378,8 +378,10 @@ constexpr int kGemmAPT = kGemmRows * kGemmBK / kGemmThreads;  // A elements per 
 constexpr int kGemmBPT = kGemmBN * kGemmBK / kGemmThreads;    // B elements per thread per slice
 
 __global__ void __launch_bounds__(kGemmThreads, 1) gemm_fp64_dmma_kernel(GemmArgs g, int mrows) {
-  __shared__ double As[kGemmBK][kGemmRows + 2];
-  __shared__ double Bs[kGemmBN][kGemmBK + 1];
+  // strides = 8 and 4 (mod 16) doubles: the fragment reads of a warp then hit
+  // every bank pair exactly twice (the minimum for 32 doubles)
+  __shared__ double As[kGemmBK][kGemmRows + 8];
+  __shared__ double Bs[kGemmBN][kGemmBK + 4];
   __shared__ int boff_s[kGemmBN];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
@@ -465,7 +467,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_fp64_dmma_kernel(GemmArg
 // Spectra are stored frequency-blocked: spec[(fb * nn + node) * kFB + f % kFB]
 // with fb = f / kFB, so one block of frequencies for every box (nn * 256 B)
 // is contiguous and stays resident in L2 while the Hadamard kernel works on it.
-constexpr int kFB = 8;
+constexpr int kFB = 32;
 __host__ __device__ __forceinline__ size_t spec_index(int f, int node, int nn) {
   return ((size_t)(f / kFB) * nn + node) * kFB + (f % kFB);
 }
@@ -664,20 +666,20 @@ struct HadamardParams {
   const int* win;      // ngroups x 216 node ids (-1 = absent)
   const int* members;  // ngroups x 8 node ids (-1 = no V list)
   // 343 x Fpad translation spectra, zero for |delta|_inf <= 1 and f >= F:
-  // double2 (FP64) or float4 {tr, tr, -ti, ti} (mixed, packed operands)
+  // double2 (FP64) or float2 (mixed)
   const void* trans;
   int Fpad;
   const void* spec;  // blocked layout, double2 or float2
   void* effv;        // blocked layout, double2 or float2
 };
 
-constexpr int kHadThreads = 256;  // 32 groups in flight x 8 frequencies
-constexpr int kHadGroupsInFlight = kHadThreads / kFB;
-constexpr int kHadGroupsPerBlock = 64;
+constexpr int kHadThreads = 256;  // 8 warps, one group per warp, lane = frequency
+constexpr int kHadGroupsInFlight = kHadThreads / 32;
+constexpr int kHadGroupsPerBlock = 32;
 
 template <bool kMixed>
 __host__ __device__ constexpr size_t had_smem_bytes() {
-  return (kMixed ? sizeof(float4) : sizeof(double2)) * 343 * kFB;
+  return (kMixed ? sizeof(float2) : sizeof(double2)) * 343 * kFB;
 }
 
 __device__ __forceinline__ void cmac64(double& ar, double& ai, const double2 t, const double2 s) {
@@ -687,12 +689,13 @@ __device__ __forceinline__ void cmac64(double& ar, double& ai, const double2 t, 
   ai = fma(t.y, s.x, ai);
 }
 
-// acc {re, im} += t * s with packed FP32: t = {tr, tr, -ti, ti}, s = {sr, si},
-// sw = {si, sr}.
-__device__ __forceinline__ unsigned long long cmac32x2(unsigned long long acc, const float4 t,
+// acc {re, im} += t * s with packed FP32: t01 = {tr, tr}, t23 = {-ti, ti},
+// s = {sr, si}, sw = {si, sr}.
+__device__ __forceinline__ unsigned long long cmac32x2(unsigned long long acc,
+                                                       unsigned long long t01,
+                                                       unsigned long long t23,
                                                        unsigned long long s,
                                                        unsigned long long sw) {
-  const unsigned long long t01 = pack2(t.x, t.y), t23 = pack2(t.z, t.w);
   asm("fma.rn.f32x2 %0, %1, %2, %0;\n"
       "fma.rn.f32x2 %0, %3, %4, %0;\n"
       : "+l"(acc)
@@ -718,30 +721,29 @@ __device__ __forceinline__ void two_sum32x2(unsigned long long& hi, unsigned lon
       : "l"(b));
 }
 
-// One block: one frequency block (blockIdx.y) for groups_per_block groups.
-// Thread (slot, f) owns all 8 members of its group at frequency f; a warp
-// holds 4 groups at the same 8 frequencies, so every translation load is
-// shared by 4 groups.  The 343 translation spectra of the frequency block sit
+// One block: one block of 32 frequencies (blockIdx.y) for groups_per_block
+// groups.  Warp = one group, lane = one frequency, all 8 members of the group
+// in registers; every shared or global load of a warp is 32 distinct,
+// contiguous values.  The 343 translation spectra of the frequency block sit
 // in shared memory (zero at the adjacent offsets: every window entry is a
 // plain multiply-add).  The window is walked row by row in x: a row of 6
 // source spectra meets, for each of the 4 (cy, cz) member pairs, one row of 7
 // translation spectra: 12 complex multiply-adds per 7 shared loads; the next
-// row's source spectra are fetched while the current row is multiplied.
-// The FP32 instance (mixed form) uses packed f32x2 multiply-adds and adds
-// each member's two-row partial sums into a two-sum (hi, lo) pair.
+// row's source spectra are fetched while the current row is multiplied.  The
+// FP32 instance (mixed form) uses packed f32x2 multiply-adds and adds each
+// member's two-row partial sums into a two-sum (hi, lo) pair.
 template <bool kMixed>
 __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p) {
   extern __shared__ __align__(16) unsigned char had_dyn[];
   __shared__ int win[kHadGroupsInFlight][216];
   __shared__ int mem[kHadGroupsInFlight][8];
   using C = typename std::conditional<kMixed, float2, double2>::type;
-  using TT = typename std::conditional<kMixed, float4, double2>::type;
-  TT* tsm = (TT*)had_dyn;  // [343][kFB]
+  C* tsm = (C*)had_dyn;  // [343][kFB]
   const C* spec = (const C*)p.spec;
-  const TT* trans = (const TT*)p.trans;
+  const C* trans = (const C*)p.trans;
   C* effv = (C*)p.effv;
   const int fb = blockIdx.y;
-  const int f = threadIdx.x % kFB, slot = threadIdx.x / kFB;
+  const int f = threadIdx.x & 31, slot = threadIdx.x >> 5;
   for (int q = threadIdx.x; q < 343 * kFB; q += kHadThreads)
     tsm[q] = trans[(size_t)(q / kFB) * p.Fpad + fb * kFB + (q % kFB)];
   const int g0 = blockIdx.x * p.groups_per_block;
@@ -758,6 +760,7 @@ __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p)
       mem[q / 8][q % 8] = g < g1 ? p.members[(size_t)g * 8 + q % 8] : -1;
     }
     __syncthreads();
+    if (gb + slot >= g1) continue;  // warp-uniform: no group for this warp
     const int* w = win[slot];
     C nxt[6];
 #pragma unroll
@@ -787,16 +790,20 @@ __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p)
 #pragma unroll
         for (int cyz = 0; cyz < 4; ++cyz) {
           const int cy = cyz >> 1, cz = cyz & 1;
-          const TT* trow = tsm + ((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * kFB + f;
-          TT t[7];
+          const C* trow = tsm + ((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * kFB + f;
+          unsigned long long t01[7], t23[7];
 #pragma unroll
-          for (int k = 0; k < 7; ++k) t[k] = trow[k * kFB];
+          for (int k = 0; k < 7; ++k) {
+            const C t = trow[k * kFB];
+            t01[k] = pack2(t.x, t.x);
+            t23[k] = pack2(-t.y, t.y);
+          }
 #pragma unroll
           for (int wx = 0; wx < 6; ++wx)
 #pragma unroll
             for (int cx = 0; cx < 2; ++cx) {
               const int c = cx * 4 + cy * 2 + cz;
-              acc[c] = cmac32x2(acc[c], t[wx - cx + 1], sr[wx], sw[wx]);
+              acc[c] = cmac32x2(acc[c], t01[wx - cx + 1], t23[wx - cx + 1], sr[wx], sw[wx]);
             }
         }
         if (row & 1) {
@@ -833,8 +840,8 @@ __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p)
 #pragma unroll
         for (int cyz = 0; cyz < 4; ++cyz) {
           const int cy = cyz >> 1, cz = cyz & 1;
-          const TT* trow = tsm + ((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * kFB + f;
-          TT t[7];
+          const C* trow = tsm + ((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * kFB + f;
+          C t[7];
 #pragma unroll
           for (int k = 0; k < 7; ++k) t[k] = trow[k * kFB];
 #pragma unroll

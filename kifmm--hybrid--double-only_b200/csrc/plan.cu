@@ -332,14 +332,12 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   p->Fpad = (F + kFB - 1) / kFB * kFB;
   p->cplx = p->prec == KFMM_MIXED ? sizeof(float2) : sizeof(double2);
   if (p->prec == KFMM_MIXED) {
-    std::vector<float4> tr((size_t)343 * p->Fpad, make_float4(0.f, 0.f, 0.f, 0.f));
+    std::vector<float2> tr((size_t)343 * p->Fpad, make_float2(0.f, 0.f));
     for (int id = 0; id < 343; ++id)
-      for (int f = 0; f < F; ++f) {
-        const float re = (float)op.ue2dc[2 * ((size_t)id * F + f)];
-        const float im = (float)op.ue2dc[2 * ((size_t)id * F + f) + 1];
-        tr[(size_t)id * p->Fpad + f] = make_float4(re, re, -im, im);
-      }
-    float4* d = nullptr;
+      for (int f = 0; f < F; ++f)
+        tr[(size_t)id * p->Fpad + f] = make_float2((float)op.ue2dc[2 * ((size_t)id * F + f)],
+                                                   (float)op.ue2dc[2 * ((size_t)id * F + f) + 1]);
+    float2* d = nullptr;
     KF_TRY(upload(p, &d, tr));
     p->d_trans = d;
   } else {
