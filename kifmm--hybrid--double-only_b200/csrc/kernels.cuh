@@ -190,16 +190,25 @@ __device__ __forceinline__ void pairs_mixed(const unsigned long long (&tx)[NP2],
   int k = 0;
   while (k < cnt) {
     const int m = min(8, cnt - k);
-    unsigned long long blk[NP2];
+    unsigned long long blk[NP2], blk2[NP2];
 #pragma unroll
-    for (int t = 0; t < NP2; ++t) blk[t] = 0ull;
+    for (int t = 0; t < NP2; ++t) blk[t] = blk2[t] = 0ull;
     if (m == 8) {
+      // even and odd sources feed separate partial sums: two independent
+      // chains behind every reciprocal square root
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < 8; u += 2) {
         const ulonglong2 a = buf[2 * (k + u)], b = buf[2 * (k + u) + 1];
+        const ulonglong2 a2 = buf[2 * (k + u + 1)], b2 = buf[2 * (k + u + 1) + 1];
 #pragma unroll
-        for (int t = 0; t < NP2; ++t) blk[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a, b, blk[t]);
+        for (int t = 0; t < NP2; ++t) {
+          blk[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a, b, blk[t]);
+          blk2[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a2, b2, blk2[t]);
+        }
       }
+#pragma unroll
+      for (int t = 0; t < NP2; ++t)
+        asm("add.f32x2 %0, %0, %1;\n" : "+l"(blk[t]) : "l"(blk2[t]));
     } else {
       for (int u = 0; u < m; ++u) {
         const ulonglong2 a = buf[2 * (k + u)], b = buf[2 * (k + u) + 1];
@@ -679,7 +688,7 @@ constexpr int kHadGroupsPerBlock = 32;
 
 template <bool kMixed>
 __host__ __device__ constexpr size_t had_smem_bytes() {
-  return (kMixed ? sizeof(float2) : sizeof(double2)) * 343 * kFB;
+  return kMixed ? sizeof(float2) * 343 * kFB : 0;
 }
 
 __device__ __forceinline__ void cmac64(double& ar, double& ai, const double2 t, const double2 s) {
@@ -738,14 +747,18 @@ __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p)
   __shared__ int win[kHadGroupsInFlight][216];
   __shared__ int mem[kHadGroupsInFlight][8];
   using C = typename std::conditional<kMixed, float2, double2>::type;
-  C* tsm = (C*)had_dyn;  // [343][kFB]
   const C* spec = (const C*)p.spec;
   const C* trans = (const C*)p.trans;
   C* effv = (C*)p.effv;
   const int fb = blockIdx.y;
   const int f = threadIdx.x & 31, slot = threadIdx.x >> 5;
-  for (int q = threadIdx.x; q < 343 * kFB; q += kHadThreads)
-    tsm[q] = trans[(size_t)(q / kFB) * p.Fpad + fb * kFB + (q % kFB)];
+  // FP32: the frequency block's translation spectra in shared memory
+  // (343 x 32 x 8 B); FP64 reads them through L1 (the 176 KB tile would
+  // leave room for one block per SM)
+  C* tsm = (C*)had_dyn;
+  if (kMixed)
+    for (int q = threadIdx.x; q < 343 * kFB; q += kHadThreads)
+      tsm[q] = trans[(size_t)(q / kFB) * p.Fpad + fb * kFB + (q % kFB)];
   const int g0 = blockIdx.x * p.groups_per_block;
   const int g1 = min(p.ngroups, g0 + p.groups_per_block);
   const size_t fbase = (size_t)fb * p.nn;
@@ -840,10 +853,12 @@ __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p)
 #pragma unroll
         for (int cyz = 0; cyz < 4; ++cyz) {
           const int cy = cyz >> 1, cz = cyz & 1;
-          const C* trow = tsm + ((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * kFB + f;
+          const C* trow =
+              trans + (size_t)((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * p.Fpad +
+              fb * kFB + f;
           C t[7];
 #pragma unroll
-          for (int k = 0; k < 7; ++k) t[k] = trow[k * kFB];
+          for (int k = 0; k < 7; ++k) t[k] = __ldg(trow + (size_t)k * p.Fpad);
 #pragma unroll
           for (int wx = 0; wx < 6; ++wx)
 #pragma unroll
