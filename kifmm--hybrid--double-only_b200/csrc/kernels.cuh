@@ -190,25 +190,16 @@ __device__ __forceinline__ void pairs_mixed(const unsigned long long (&tx)[NP2],
   int k = 0;
   while (k < cnt) {
     const int m = min(8, cnt - k);
-    unsigned long long blk[NP2], blk2[NP2];
+    unsigned long long blk[NP2];
 #pragma unroll
-    for (int t = 0; t < NP2; ++t) blk[t] = blk2[t] = 0ull;
+    for (int t = 0; t < NP2; ++t) blk[t] = 0ull;
     if (m == 8) {
-      // even and odd sources feed separate partial sums: two independent
-      // chains behind every reciprocal square root
-#pragma unroll
-      for (int u = 0; u < 8; u += 2) {
+#pragma unroll 4
+      for (int u = 0; u < 8; ++u) {
         const ulonglong2 a = buf[2 * (k + u)], b = buf[2 * (k + u) + 1];
-        const ulonglong2 a2 = buf[2 * (k + u + 1)], b2 = buf[2 * (k + u + 1) + 1];
 #pragma unroll
-        for (int t = 0; t < NP2; ++t) {
-          blk[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a, b, blk[t]);
-          blk2[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a2, b2, blk2[t]);
-        }
+        for (int t = 0; t < NP2; ++t) blk[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a, b, blk[t]);
       }
-#pragma unroll
-      for (int t = 0; t < NP2; ++t)
-        asm("add.f32x2 %0, %0, %1;\n" : "+l"(blk[t]) : "l"(blk2[t]));
     } else {
       for (int u = 0; u < m; ++u) {
         const ulonglong2 a = buf[2 * (k + u)], b = buf[2 * (k + u) + 1];
@@ -331,7 +322,7 @@ __device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, in
 }
 
 template <bool kMixed, int kMaxSlots>
-__global__ void __launch_bounds__(32 * kWarpJobsPerBlock, 4)
+__global__ void __launch_bounds__(32 * kWarpJobsPerBlock, kMixed ? 6 : 4)
 p2p_warp_kernel(P2PParams p, int njobs) {
   __shared__ __align__(16) unsigned char smem[kWarpJobsPerBlock][32 * 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
