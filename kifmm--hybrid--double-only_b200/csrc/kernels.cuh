@@ -351,6 +351,8 @@ p2p_warp_kernel(P2PParams p, int njobs) {
 struct GemmArgs {
   const double* A;
   int M, K;
+  int ksplit;        // K range per blockIdx.z (multiple of kGemmBK)
+  double* partial;   // split-K: partial sums [z][ncol][M] (no alpha), else NULL
   const double* B;
   const int* boff;
   double* C;
@@ -387,6 +389,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_fp64_dmma_kernel(GemmArg
   const int wm = warp >> 1, wn = warp & 1;
   const int m0 = blockIdx.x * mrows, n0 = blockIdx.y * kGemmBN;
   const int mend = min(g.M, m0 + mrows);
+  const int kb = blockIdx.z * g.ksplit, ke = min(g.K, kb + g.ksplit);
   if (tid < kGemmBN) boff_s[tid] = (n0 + tid < g.ncol) ? g.boff[n0 + tid] : -1;
   double acc[5][4][2];
 #pragma unroll
@@ -401,18 +404,18 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_fp64_dmma_kernel(GemmArg
       const int idx = tid + r * kGemmThreads;
       const int m = idx % kGemmRows, k = idx / kGemmRows;
       const int gm = m0 + m, gk = k0 + k;
-      ra[r] = (gm < mend && gk < g.K) ? g.A[(size_t)gk * g.M + gm] : 0.0;
+      ra[r] = (gm < mend && gk < ke) ? g.A[(size_t)gk * g.M + gm] : 0.0;
     }
 #pragma unroll
     for (int r = 0; r < kGemmBPT; ++r) {
       const int idx = tid + r * kGemmThreads;
       const int k = idx % kGemmBK, n = idx / kGemmBK;
       const int gk = k0 + k, bo = boff_s[n];
-      rb[r] = (bo >= 0 && gk < g.K) ? g.B[(size_t)bo + gk] : 0.0;
+      rb[r] = (bo >= 0 && gk < ke) ? g.B[(size_t)bo + gk] : 0.0;
     }
   };
-  fetch(0);
-  for (int k0 = 0; k0 < g.K; k0 += kGemmBK) {
+  fetch(kb);
+  for (int k0 = kb; k0 < ke; k0 += kGemmBK) {
 #pragma unroll
     for (int r = 0; r < kGemmAPT; ++r) {
       const int idx = tid + r * kGemmThreads;
@@ -424,7 +427,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_fp64_dmma_kernel(GemmArg
       Bs[idx / kGemmBK][idx % kGemmBK] = rb[r];
     }
     __syncthreads();
-    if (k0 + kGemmBK < g.K) fetch(k0 + kGemmBK);
+    if (k0 + kGemmBK < ke) fetch(k0 + kGemmBK);
 #pragma unroll
     for (int kk = 0; kk < kGemmBK; kk += 4) {
       double af[5], bf[4];
@@ -449,13 +452,34 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_fp64_dmma_kernel(GemmArg
         const int m = m0 + wm * 40 + mi * 8 + (lane >> 2);
         const int n = n0 + wn * 32 + ni * 8 + (lane & 3) * 2 + h;
         if (m < mend && n < g.ncol) {
-          const double a = g.alpha ? g.alpha[n] : g.alpha_const;
-          double* c = g.C + (size_t)g.coff[n] + m;
-          const double v = a * acc[mi][ni][h];
-          if (g.accumulate) *c += v;
-          else *c = v;
+          if (g.partial) {
+            g.partial[((size_t)blockIdx.z * g.ncol + n) * g.M + m] = acc[mi][ni][h];
+          } else {
+            const double a = g.alpha ? g.alpha[n] : g.alpha_const;
+            double* c = g.C + (size_t)g.coff[n] + m;
+            const double v = a * acc[mi][ni][h];
+            if (g.accumulate) *c += v;
+            else *c = v;
+          }
         }
       }
+}
+
+// Split-K: sum the partial products in split order (deterministic), then
+// scale and store as the single-pass kernel would.
+__global__ void gemm_splitk_reduce_kernel(GemmArgs g, int nsplit) {
+  const size_t total = (size_t)g.ncol * g.M;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < total;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int n = (int)(q / g.M), m = (int)(q % g.M);
+    double sum = 0.0;
+    for (int z = 0; z < nsplit; ++z) sum += g.partial[((size_t)z * g.ncol + n) * g.M + m];
+    const double a = g.alpha ? g.alpha[n] : g.alpha_const;
+    double* c = g.C + (size_t)g.coff[n] + m;
+    const double v = a * sum;
+    if (g.accumulate) *c += v;
+    else *c = v;
+  }
 }
 
 // ---------------------------------------------------------------------------

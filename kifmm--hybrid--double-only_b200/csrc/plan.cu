@@ -51,6 +51,7 @@ void set_error(const std::string& msg) { g_error = msg; }
 struct GemmBatch {
   const double* A;
   int M, K;
+  int chunks, mrows, nsplit, ksplit;  // launch shape, fixed at plan time
   const double* B;
   int* boff;  // device
   double* C;
@@ -99,6 +100,9 @@ struct kfmm_plan {
   int *win = nullptr, *members = nullptr;
   int n_groups = 0;
   kfmm_stats stats{};
+  int num_sms = 148;
+  double* splitk = nullptr;   // split-K partial sums, shared by the level GEMMs
+  size_t splitk_doubles = 0;
   bool timing = false;
   cudaEvent_t ev[7] = {};
   float phase_ms[6] = {};
@@ -152,23 +156,36 @@ kfmm_status add_gemm(kfmm_plan* p, std::vector<GemmBatch>& out, const double* A,
   KF_TRY(upload(p, &g.boff, boff));
   KF_TRY(upload(p, &g.coff, coff));
   if (alpha) KF_TRY(upload(p, &g.alpha, *alpha));
+  // rows in near-equal chunks of <= kGemmRows (multiples of 8); split K when
+  // the launch would give fewer than two blocks per SM
+  g.chunks = (M + kGemmRows - 1) / kGemmRows;
+  g.mrows = ((M + g.chunks - 1) / g.chunks + 7) / 8 * 8;
+  const int blocks = g.chunks * ((g.ncol + kGemmBN - 1) / kGemmBN);
+  const int want = 2 * p->num_sms;
+  g.nsplit = 1;
+  if (blocks < want) g.nsplit = std::max(1, std::min((want + blocks - 1) / blocks, K / 64));
+  g.ksplit = ((K + g.nsplit - 1) / g.nsplit + kGemmBK - 1) / kGemmBK * kGemmBK;
+  g.nsplit = (K + g.ksplit - 1) / g.ksplit;
+  if (g.nsplit > 1)
+    p->splitk_doubles = std::max(p->splitk_doubles, (size_t)g.nsplit * g.ncol * M);
   p->stats.gemm_flops += 2.0 * M * (double)K * g.ncol;
   out.push_back(g);
   return KFMM_OK;
 }
 
-kfmm_status launch_gemms(const std::vector<GemmBatch>& gs, size_t first, size_t last,
-                         cudaStream_t st) {
-  for (size_t i = first; i < last; ++i) {
-    const GemmBatch& b = gs[i];
-    GemmArgs a{b.A, b.M, b.K, b.B, b.boff, b.C, b.coff, b.alpha, b.alpha_const, b.ncol,
-               b.accumulate};
-    // split the M rows into near-equal chunks of <= kGemmRows, multiples of 8
-    const int chunks = (b.M + kGemmRows - 1) / kGemmRows;
-    const int mrows = ((b.M + chunks - 1) / chunks + 7) / 8 * 8;
-    dim3 grid(chunks, (b.ncol + kGemmBN - 1) / kGemmBN);
-    gemm_fp64_dmma_kernel<<<grid, kGemmThreads, 0, st>>>(a, mrows);
+kfmm_status launch_gemms(const kfmm_plan* p, const std::vector<GemmBatch>& gs, cudaStream_t st) {
+  for (const GemmBatch& b : gs) {
+    GemmArgs a{b.A, b.M, b.K, b.ksplit, b.nsplit > 1 ? p->splitk : nullptr, b.B, b.boff, b.C,
+               b.coff, b.alpha, b.alpha_const, b.ncol, b.accumulate};
+    dim3 grid(b.chunks, (b.ncol + kGemmBN - 1) / kGemmBN, b.nsplit);
+    gemm_fp64_dmma_kernel<<<grid, kGemmThreads, 0, st>>>(a, b.mrows);
     KF_CHECK_LAUNCH("gemm_fp64_dmma_kernel");
+    if (b.nsplit > 1) {
+      const size_t total = (size_t)b.ncol * b.M;
+      const int blocks = (int)std::min<size_t>((total + 255) / 256, 4 * (size_t)p->num_sms);
+      gemm_splitk_reduce_kernel<<<blocks, 256, 0, st>>>(a, b.nsplit);
+      KF_CHECK_LAUNCH("gemm_splitk_reduce_kernel");
+    }
   }
   return KFMM_OK;
 }
@@ -274,6 +291,11 @@ inline long long key_of(int x, int y, int z) {
 
 kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operator_set* user) {
   const int nn = d->num_nodes, np = p->np;
+  {
+    int dev = 0;
+    KF_CUDA(cudaGetDevice(&dev));
+    KF_CUDA(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev));
+  }
   Operators op = operators_for(np);
   if (user) {
     const size_t P0 = op.P, Q0 = op.Q;
@@ -455,7 +477,10 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       if (!is_leaf(i) && has_src(i)) par[d->depth[i]].push_back(i);
     for (int dd = 0; dd <= maxd; ++dd) maxpar = std::max(maxpar, (int)par[dd].size());
     KF_TRY(dalloc(p, &p->chk_m, (size_t)maxpar * Q));
-    for (int dd = maxd - 1; dd >= 0; --dd) {
+    // Equivalent densities of depth 0 and 1 nodes are never read: V lists
+    // start at depth 2 and W-list nodes lie below a depth >= 1 leaf's
+    // colleagues, so at depth >= 2.  M2M stops at parents of depth 2.
+    for (int dd = maxd - 1; dd >= 2; --dd) {
       if (par[dd].empty()) continue;
       std::vector<int> b1, c1, b2, c2;
       for (size_t k = 0; k < par[dd].size(); ++k) {
@@ -612,11 +637,15 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_CUDA(cudaFuncSetAttribute(hadamard_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)had_smem_bytes<true>()));
 
+  if (p->splitk_doubles) KF_TRY(dalloc(p, &p->splitk, p->splitk_doubles));
   p->stats.num_nodes = nn;
   p->stats.P = P;
   p->stats.Q = Q;
   p->stats.F = F;
-  p->stats.launches = (p->n_s2m > 0) + (int)p->up_gemms.size() + (p->n_fft > 0) +
+  int reduces = 0;
+  for (const GemmBatch& b : p->up_gemms) reduces += b.nsplit > 1;
+  for (const GemmBatch& b : p->down_gemms) reduces += b.nsplit > 1;
+  p->stats.launches = reduces + (p->n_s2m > 0) + (int)p->up_gemms.size() + (p->n_fft > 0) +
                       (p->n_groups > 0) + (p->n_ifft > 0) + (p->n_s2l > 0) +
                       (int)p->down_gemms.size() + (p->n_nf > 0) + 1;
   for (int i = 0; i < 7; ++i) KF_CUDA(cudaEventCreate(&p->ev[i]));
@@ -778,7 +807,7 @@ kfmm_status kfmm_up_calc(kfmm_plan* p, void* stream) {
     KF_TRY(launch_p2p(p, p->n_s2m, p2p_params(p, p->s2m_jobs, p->s2m_ent, p->chk_up), stream,
                       "s2m"));
   }
-  return launch_gemms(p->up_gemms, 0, p->up_gemms.size(), S(stream));
+  return launch_gemms(p, p->up_gemms, S(stream));
 }
 
 kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
@@ -822,7 +851,7 @@ kfmm_status kfmm_xlist_calc(kfmm_plan* p, void* stream) {
 
 kfmm_status kfmm_down_calc(kfmm_plan* p, void* stream) {
   if (!p) return KFMM_ERR_INVALID;
-  return launch_gemms(p->down_gemms, 0, p->down_gemms.size(), S(stream));
+  return launch_gemms(p, p->down_gemms, S(stream));
 }
 
 kfmm_status kfmm_ulist_calc(kfmm_plan* p, void* stream) {

@@ -84,8 +84,49 @@ static void localpos(const oracle_tree* t, int node, const double* sp, int n, do
   }
 }
 
+/* Precision of the operator products (matrix-vector products with the
+ * translation operators): 0 FP64 (the reference), 1 FP32 inputs and FP32
+ * accumulation, 2 split-TF32 three-pass products (hi*hi + hi*lo + lo*hi,
+ * 10-bit mantissas) accumulated in FP32.  Modes 1 and 2 exist to measure what
+ * reduced-precision level products would do to the potentials. */
+static int g_prod = 0;
+void oracle_set_product_precision(int mode) { g_prod = mode; }
+
+static float round_tf32(float x) {
+  unsigned u;
+  memcpy(&u, &x, 4);
+  u = (u + 0x1000u) & 0xffffe000u; /* round to 10 explicit mantissa bits */
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
+static void gemv_reduced(int m, int n, const double* A, const double* x, double* y) {
+  float* acc = (float*)calloc(m, sizeof(float));
+  for (int j = 0; j < n; j++) {
+    float xj = (float)x[j];
+    const double* a = A + (size_t)j * m;
+    for (int i = 0; i < m; i++) {
+      float ai = (float)a[i];
+      if (g_prod == 1) {
+        acc[i] = fmaf(xj, ai, acc[i]);
+      } else {
+        float ah = round_tf32(ai), al = round_tf32(ai - ah);
+        float xh = round_tf32(xj), xl = round_tf32(xj - xh);
+        acc[i] += ah * xh + (ah * xl + al * xh);
+      }
+    }
+  }
+  for (int i = 0; i < m; i++) y[i] += acc[i];
+  free(acc);
+}
+
 /* y += A x, A m x n column-major (dgemv, fmm/vecmatop.cc:15-22) */
 static void gemv(int m, int n, const double* A, const double* x, double* y) {
+  if (g_prod) {
+    gemv_reduced(m, n, A, x, y);
+    return;
+  }
   for (int jj = 0; jj < n; jj++) {
     int j = g_reverse ? n - 1 - jj : jj;
     double xj = x[j];

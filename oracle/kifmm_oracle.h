@@ -40,6 +40,12 @@ int oracle_evaluate(const oracle_tree* t, int np, const oracle_ops* ops, const d
  * measure the algorithm's own rounding floor).  Process-wide. */
 void oracle_set_order(int reverse);
 
+/* Precision of the operator matrix-vector products: 0 FP64 (reference),
+ * 1 FP32, 2 split-TF32 three-pass with FP32 accumulation.  Process-wide;
+ * used to measure the sensitivity of the potentials to reduced-precision
+ * level products. */
+void oracle_set_product_precision(int mode);
+
 /* ulist__direct_evaluation over all sources for selected targets (the check of
  * fmm/driver.cc:142-206 with a zeroed accumulator). */
 void oracle_direct(int nt, const double* tx, const double* ty, const double* tz, int ns,

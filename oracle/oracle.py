@@ -47,6 +47,8 @@ def lib():
         L.oracle_direct.restype = None
         L.oracle_set_order.argtypes = [ctypes.c_int]
         L.oracle_set_order.restype = None
+        L.oracle_set_product_precision.argtypes = [ctypes.c_int]
+        L.oracle_set_product_precision.restype = None
         _lib = L
     return _lib
 
@@ -91,6 +93,16 @@ def evaluate_reordered(tree, np_, ops, pts):
         return evaluate(tree, np_, ops, pts)
     finally:
         lib().oracle_set_order(0)
+
+
+def evaluate_reduced_products(tree, np_, ops, pts, mode):
+    """The oracle with its operator matrix-vector products in FP32 (mode 1)
+    or split-TF32 three-pass with FP32 accumulation (mode 2)."""
+    lib().oracle_set_product_precision(mode)
+    try:
+        return evaluate(tree, np_, ops, pts)
+    finally:
+        lib().oracle_set_product_precision(0)
 
 
 def direct(tx, ty, tz, sx, sy, sz, den):

@@ -70,7 +70,8 @@ def test_plain_fp64_vs_oracle(K, oracle_mod, cuda_ok, case):
     P, _, _ = K.sizes(np_)
     nn = tree.desc.num_nodes
     tag = tarrs["tag"]
-    src_nodes = np.where(tag & 1)[0]
+    # equivalent densities above depth 2 are never read and not computed
+    src_nodes = np.where((tag & 1) & (tarrs["depth"] >= 2))[0]
     trg_nodes = np.where(tag & 2)[0]
     e_ud = _node_err(plan.read(0, nn * P), ud, P, src_nodes)
     e_dc = _node_err(plan.read(1, nn * P), dc, P, trg_nodes)
