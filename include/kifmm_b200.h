@@ -182,6 +182,28 @@ kfmm_status kfmm_plan_stats(const kfmm_plan* plan, kfmm_stats* stats);
 kfmm_status kfmm_enable_timing(kfmm_plan* plan, int enable);
 kfmm_status kfmm_phase_times(const kfmm_plan* plan, float* ms6);
 
+/* Allocation-free S2M for a batch of leaves; it has no counterpart in the
+ * reference.  For callers that may not allocate device memory at call time
+ * (a host framework that owns all device memory through its own pool, or a
+ * solver step run while such a framework holds the memory budget):
+ * everything is passed in, and the only scratch, the leaves' check
+ * potentials, lives in a fixed 8 MiB array inside the library image (one per
+ * GPU that loads the library, resident until the process exits).
+ *   src4     device, leaf-ordered sources as (x, y, z, w) quadruples
+ *   leaf_beg, leaf_num  device, each leaf's source range in src4
+ *   leaf_ctr device, 4 doubles per leaf: centre x, y, z and radius 2^-depth
+ *   uc2ue    device, the P x Q UC2UE operator (column-major, kfmm_operators)
+ *   uden     device output, nleaves x P upward equivalent densities
+ * Limit: nleaves * Q <= 1,048,576 (3542 leaves at NP=6); larger batches are
+ * rejected with KFMM_ERR_INVALID.  The first call on a device sets that
+ * device up (symbol addresses, a small surface table, synchronous) and should
+ * come before any stream capture.  All calls on a device share the scratch:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * No cudaMalloc/cudaFree or allocating library call is made. */
+kfmm_status kfmm_s2m_noalloc(int np, int nleaves, const double* src4, const int* leaf_beg,
+                             const int* leaf_num, const double* leaf_ctr, const double* uc2ue,
+                             double* uden, void* stream);
+
 /* Throughput of the current device's execution pipes, measured by
  * micro-benchmarks (no reference counterpart; roofline denominators):
  * what 0: FP64 FMA TFLOP/s, 1: FP32 FMA TFLOP/s, 2: FP32 rsqrt 1e12/s (MUFU),

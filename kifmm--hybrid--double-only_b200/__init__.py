@@ -89,6 +89,7 @@ def lib():
         "kfmm_enable_timing": [vp, i],
         "kfmm_phase_times": [vp, ctypes.POINTER(ctypes.c_float)],
         "kfmm_measure_peak": [i, _f64p],
+        "kfmm_s2m_noalloc": [i, i, vp, vp, vp, vp, vp, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
