@@ -51,9 +51,9 @@ def build(verbose=False, force=False):
             os.remove(o)
     cli_src = os.path.join(CSRC, "fmmd_b200.cc")
     if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB])):
-        _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),
-              cli_src, "-o", CLI, "-L", HERE, "-l:libkifmm_b200.so", "-Wl,-rpath,$ORIGIN",
-              "-lm"], verbose)
+        _run([NVCC] + ARCH + ["-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-Xcompiler",
+              "-ffp-contract=off", cli_src, "-o", CLI, "-L", HERE, "-l:libkifmm_b200.so",
+              "-Xlinker", "-rpath,$ORIGIN", "-lm"], verbose)
     return LIB
 
 
