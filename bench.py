@@ -34,6 +34,11 @@ METRIC = "Mpts/s per FMM solve at 4M pts NP=6, mixed vs FP64 on B200, rel-L2 err
 WORKLOAD = "KIFMM Laplace solve, 4194304 uniform points, NP=6, 512 pts/box"
 CPU_SAMPLE_N = 1048576  # bounded sample for the CPU reference (same NP, leaf size, generator)
 FLOPS_PER_PAIR = 11.0   # reference convention, fmm/driver.cc:60
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one near-field
+# launch at this workload, from one ncu capture per form on a B200 of this
+# pool; the algorithmic bytes (sources, targets, potentials and downward
+# densities once each) are 348 MB.
+NEAR_FIELD_DRAM_BYTES = {"mixed": 354.8e6, "fp64": 357.1e6}
 
 
 def parse():
@@ -320,7 +325,9 @@ def main():
             bound, kern = "fp64 rsqrt", "p2p_warp_kernel<fp64> (near field: U+W+X+L2T)"
         return {"bound": bound, "kernel": kern,
                 "achieved": FLOPS_PER_PAIR * rate / 1e12, "peak": FLOPS_PER_PAIR * ceil / 1e12,
-                "unit": "TFLOP/s", "frac": rate / ceil, "traffic": None,
+                "unit": "TFLOP/s", "frac": rate / ceil,
+                "traffic": NEAR_FIELD_DRAM_BYTES[name] if n == N_POINTS else None,
+                "algorithmic_bytes": 32.0 * n + 32.0 * n + 8.0 * n + 8.0 * st["num_nodes"] * st["P"],
                 "algorithmic": f"{FLOPS_PER_PAIR:g} flops/pair (fmm/driver.cc:60) x {pairs:.4e} "
                                "pairs per launch; peak = one pair per measured reciprocal-sqrt "
                                "issue",

@@ -6,6 +6,11 @@ the GPU evaluator; fmmd--b200 is this repository's stand-alone driver with the
 same CLI and output lines.  Both must report the same "Relative error" (the
 reference's direct-sum check, fmm/driver.cc:142-206) as fmmd--omp for the same
 command line.
+
+The reference driver's check accumulates into an array it never zeroes
+(chkPot, fmm/driver.cc:157).  The reference binaries here run with
+glibc.malloc.mmap_threshold=4096 and NV >= 512, so that array (8 NV bytes)
+comes from fresh zeroed pages in every binary.
 """
 import os
 import re
@@ -50,7 +55,7 @@ CASES = [("uniform", 65536, 128, 4, 0), ("ellipseUniformAngles", 20000, 32, 3, 0
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}-{c[1]}-{c[2]}-np{c[3]}-C{c[4]}")
 def test_dropin_matches_reference_driver(case):
     dist, n, ppb, np_, c = case
-    env = {"NP": str(np_), "NV": "300", "C": str(c)}
+    env = {"NP": str(np_), "NV": "600", "C": str(c)}
     ref = run(REF_OMP, [n, dist, ppb], **env)
     assert ref.returncode == 0, ref.stderr[-500:]
     e_ref = rel_error(ref)
@@ -66,8 +71,12 @@ def test_dropin_matches_reference_driver(case):
     e_mixed = rel_error(mixed)
     print(f"{case}: reference {e_ref:.6e} drop-in {e_drop:.6e} fmmd--b200 {e_cli:.6e} "
           f"drop-in mixed {e_mixed:.6e}")
-    # same tree, operators and check: potentials differ by rounding only
-    assert abs(e_drop - e_ref) <= 1e-6 * e_ref + 1e-14
+    # |e_a - e_b| <= max per-target relative deviation of the potentials
+    # (triangle inequality), which is the FP64 rounding floor for the same
+    # operators (~0.1^-(np+1) * 1e-17, see test_gpu_parity); plus the 7
+    # significant digits the driver prints
+    floor = 1e-17 * 10.0 ** (np_ + 1) * 20
+    assert abs(e_drop - e_ref) <= 1e-6 * e_ref + floor
     # own pseudo-inverses: differences at the SVD's rounding level
-    assert abs(e_cli - e_ref) <= 1e-3 * e_ref + 1e-14
+    assert abs(e_cli - e_ref) <= 1e-6 * e_ref + 5 * floor
     assert e_mixed <= 2.0 * e_ref
