@@ -2,7 +2,8 @@
 //
 //   fmmd--b200 <#pts> {uniform,ellipseUniformAngles,ellipsoidSurface} <#pts-per-box>
 //   env NP (expansion order, default 6), NV (validation targets, default
-//   1000), C (1: targets are the sources), and KFMM_MIXED=1 for the mixed form.
+//   1000), C (1: targets are the sources), KFMM_MIXED=1 for the mixed form,
+//   KFMM_DUMP_POT=<file> to write the potentials (original order, raw doubles).
 //
 // Same sequence and output lines as fmm/driver.cc:211-371: seed 26, points,
 // densities, octree + lists, preproc, run (phase timings on stderr), then the
@@ -66,6 +67,14 @@ int main(int argc, char** argv) {
   CHECK(kfmm_enable_timing(plan, 1));
   CHECK(kfmm_evaluate(plan, sx.data(), sy.data(), sz.data(), den.data(), tx.data(), ty.data(),
                       tz.data(), pot.data(), nullptr));
+  if (const char* path = std::getenv("KFMM_DUMP_POT")) {
+    FILE* f = std::fopen(path, "wb");
+    if (!f || std::fwrite(pot.data(), sizeof(double), n, f) != (size_t)n) {
+      std::fprintf(stderr, "KFMM_DUMP_POT: cannot write %s\n", path);
+      return 1;
+    }
+    std::fclose(f);
+  }
   float ms[6];
   CHECK(kfmm_phase_times(plan, ms));
   const double t_up = ms[0] * 1e-3, t_v = ms[1] * 1e-3, t_x = ms[2] * 1e-3,

@@ -79,14 +79,21 @@ __device__ __forceinline__ void two_sum(float& hi, float& lo, float b) {
 // own, without block barriers.  Sources are fetched 32 at a time, one per lane
 // (coalesced), prepared in the lane, and written to the warp's own shared
 // buffer; after __syncwarp every lane reads each source back as a broadcast.
-// Each source then meets the lane's `slots` targets: independent dependency
-// chains per source.  r = 0 can only occur between a leaf's own sources and
-// targets (equal coordinates always fall in the same leaf), so only the
-// self entry carries the r > 0 test (fmm/omp.cc:280).
+// The next 32 sources are fetched into registers while the current ones are
+// used.  Each source then meets the lane's `slots` targets: independent
+// dependency chains per source.  r = 0 can only occur between a leaf's own
+// sources and targets (equal coordinates always fall in the same leaf), so
+// only the self entry carries the r > 0 test (fmm/omp.cc:280).
+//
+// The kernel is persistent: a grid of (SMs x resident blocks) warps takes jobs
+// from an atomic counter; the host orders the jobs by decreasing cost, so the
+// largest start first and the tail is short.
 // ---------------------------------------------------------------------------
 constexpr int kWarpJobsPerBlock = 4;
-constexpr int kMaxSlotsFP64 = 4;   // targets per lane, FP64 jobs
-constexpr int kMaxSlotsMixed = 4;  // targets per lane, mixed jobs (even: packed pairs)
+constexpr int kMaxSlots = 6;  // targets per lane: jobs hold up to 192 targets
+#ifndef KFMM_P2P_MIXED_MINB
+#define KFMM_P2P_MIXED_MINB 6  // resident blocks per SM asked of the mixed P2P kernel
+#endif
 
 __device__ __forceinline__ void load_entry_source(const P2PParams& p, int kind, int node,
                                                   int base, int idx, double3& s, double& w) {
@@ -180,38 +187,84 @@ __device__ __forceinline__ unsigned long long pair_term2(unsigned long long tx,
   return out;
 }
 
-// buf: per source {x,x},{y,y} then {z,z},{w,w} (two ulonglong2 per source)
-template <int NP2, bool kGuard>
-__device__ __forceinline__ void pairs_mixed(const unsigned long long (&tx)[NP2],
-                                            const unsigned long long (&ty)[NP2],
-                                            const unsigned long long (&tz)[NP2],
-                                            float (&hi)[2 * NP2], float (&lo)[2 * NP2],
+// Scalar FP32 pair, for the odd target of a lane with an odd slot count.
+template <bool kGuard>
+__device__ __forceinline__ float pair_term1(float tx, float ty, float tz, float sx, float sy,
+                                            float sz, float w, float blk) {
+  float out;
+  if (kGuard) {
+    asm("{\n"
+        " .reg .f32 dx, dy, dz, r2, inv;\n"
+        " .reg .pred pa;\n"
+        " sub.f32 dx, %1, %4;\n"
+        " sub.f32 dy, %2, %5;\n"
+        " sub.f32 dz, %3, %6;\n"
+        " mul.f32 r2, dx, dx;\n"
+        " fma.rn.f32 r2, dy, dy, r2;\n"
+        " fma.rn.f32 r2, dz, dz, r2;\n"
+        " rsqrt.approx.ftz.f32 inv, r2;\n"
+        " setp.gt.f32 pa, r2, 0f00000000;\n"
+        " selp.f32 inv, inv, 0f00000000, pa;\n"
+        " fma.rn.f32 %0, %7, inv, %8;\n"
+        "}\n"
+        : "=f"(out)
+        : "f"(tx), "f"(ty), "f"(tz), "f"(sx), "f"(sy), "f"(sz), "f"(w), "f"(blk));
+  } else {
+    asm("{\n"
+        " .reg .f32 dx, dy, dz, r2, inv;\n"
+        " sub.f32 dx, %1, %4;\n"
+        " sub.f32 dy, %2, %5;\n"
+        " sub.f32 dz, %3, %6;\n"
+        " mul.f32 r2, dx, dx;\n"
+        " fma.rn.f32 r2, dy, dy, r2;\n"
+        " fma.rn.f32 r2, dz, dz, r2;\n"
+        " rsqrt.approx.ftz.f32 inv, r2;\n"
+        " fma.rn.f32 %0, %7, inv, %8;\n"
+        "}\n"
+        : "=f"(out)
+        : "f"(tx), "f"(ty), "f"(tz), "f"(sx), "f"(sy), "f"(sz), "f"(w), "f"(blk));
+  }
+  return out;
+}
+
+// NS targets per lane: NS / 2 packed pairs, plus one scalar target when NS is
+// odd (the high half of the last packed register is then unused).
+// buf: per source {x,x},{y,y} then {z,z},{w,w} (two ulonglong2 per source).
+template <int NS, bool kGuard>
+__device__ __forceinline__ void pairs_mixed(const unsigned long long (&tx)[(NS + 1) / 2],
+                                            const unsigned long long (&ty)[(NS + 1) / 2],
+                                            const unsigned long long (&tz)[(NS + 1) / 2],
+                                            float (&hi)[NS], float (&lo)[NS],
                                             const ulonglong2* buf, int cnt) {
+  constexpr int NP2 = NS / 2, ODD = NS & 1;
   int k = 0;
   while (k < cnt) {
     const int m = min(8, cnt - k);
-    unsigned long long blk[NP2];
+    unsigned long long blk[NP2 > 0 ? NP2 : 1];
+    float blk1 = 0.f;
 #pragma unroll
     for (int t = 0; t < NP2; ++t) blk[t] = 0ull;
+    auto step = [&](int u) {
+      const ulonglong2 a = buf[2 * (k + u)], b = buf[2 * (k + u) + 1];
+#pragma unroll
+      for (int t = 0; t < NP2; ++t) blk[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a, b, blk[t]);
+      if (ODD)
+        blk1 = pair_term1<kGuard>(lo_of(tx[NP2]), lo_of(ty[NP2]), lo_of(tz[NP2]), lo_of(a.x),
+                                  lo_of(a.y), lo_of(b.x), lo_of(b.y), blk1);
+    };
     if (m == 8) {
-#pragma unroll 4
-      for (int u = 0; u < 8; ++u) {
-        const ulonglong2 a = buf[2 * (k + u)], b = buf[2 * (k + u) + 1];
-#pragma unroll
-        for (int t = 0; t < NP2; ++t) blk[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a, b, blk[t]);
-      }
+      constexpr int kUnroll = NS > 4 ? 2 : 4;  // bounds the live pair temporaries
+#pragma unroll kUnroll
+      for (int u = 0; u < 8; ++u) step(u);
     } else {
-      for (int u = 0; u < m; ++u) {
-        const ulonglong2 a = buf[2 * (k + u)], b = buf[2 * (k + u) + 1];
-#pragma unroll
-        for (int t = 0; t < NP2; ++t) blk[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a, b, blk[t]);
-      }
+      for (int u = 0; u < m; ++u) step(u);
     }
 #pragma unroll
     for (int t = 0; t < NP2; ++t) {
       two_sum(hi[2 * t], lo[2 * t], lo_of(blk[t]));
       two_sum(hi[2 * t + 1], lo[2 * t + 1], hi_of(blk[t]));
     }
+    if (ODD) two_sum(hi[NS - 1], lo[NS - 1], blk1);
     k += m;
   }
 }
@@ -237,42 +290,59 @@ __device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, in
     q[t][1] = v.y;
     q[t][2] = v.z;
   }
+  // chunk cursor over the job's entries: entry e, sources [c0, c0 + 32)
+  int e = J.ebeg, c0 = 0, kind = 0, node = 0, count = 0, base = 0;
+  auto open_entry = [&]() {  // first entry at or after e with sources
+    for (; e < J.eend; ++e) {
+      const int ent = p.entries[e];
+      kind = ent >> 28;
+      node = ent & 0x0fffffff;
+      count = kind == 0 ? p.src_num[node] : p.P;
+      base = kind == 0 ? p.src_beg[node] : 0;
+      if (count > 0) return;
+    }
+  };
+  open_entry();
+  double3 s = make_double3(0.0, 0.0, 0.0);
+  double w = 0.0;
+  if (e < J.eend && lane < min(32, count - c0)) load_entry_source(p, kind, node, base, c0 + lane, s, w);
+
   double sum[NS];
   if constexpr (kMixed) {
-    constexpr int NP2 = NS / 2;
-    unsigned long long tx[NP2], ty[NP2], tz[NP2];
+    constexpr int NP2C = (NS + 1) / 2;
+    unsigned long long tx[NP2C], ty[NP2C], tz[NP2C];
 #pragma unroll
-    for (int t = 0; t < NP2; ++t) {
-      tx[t] = pack2((float)(q[2 * t][0] - org.x), (float)(q[2 * t + 1][0] - org.x));
-      ty[t] = pack2((float)(q[2 * t][1] - org.y), (float)(q[2 * t + 1][1] - org.y));
-      tz[t] = pack2((float)(q[2 * t][2] - org.z), (float)(q[2 * t + 1][2] - org.z));
+    for (int t = 0; t < NP2C; ++t) {
+      const int u = 2 * t + 1 < NS ? 2 * t + 1 : 2 * t;
+      tx[t] = pack2((float)(q[2 * t][0] - org.x), (float)(q[u][0] - org.x));
+      ty[t] = pack2((float)(q[2 * t][1] - org.y), (float)(q[u][1] - org.y));
+      tz[t] = pack2((float)(q[2 * t][2] - org.z), (float)(q[u][2] - org.z));
     }
     float hi[NS], lo[NS];
 #pragma unroll
     for (int t = 0; t < NS; ++t) hi[t] = lo[t] = 0.f;
     ulonglong2* buf = (ulonglong2*)wbuf;
-    for (int e = J.ebeg; e < J.eend; ++e) {
-      const int ent = p.entries[e];
-      const int kind = ent >> 28, node = ent & 0x0fffffff;
-      const int count = kind == 0 ? p.src_num[node] : p.P;
-      const int base = kind == 0 ? p.src_beg[node] : 0;
+    while (e < J.eend) {
+      const int cnt = min(32, count - c0);
       const bool guard = kind == 0 && J.tkind == 0 && node == J.tnode;
-      for (int c0 = 0; c0 < count; c0 += 32) {
-        const int cnt = min(32, count - c0);
-        if (lane < cnt) {
-          double3 s;
-          double w;
-          load_entry_source(p, kind, node, base, c0 + lane, s, w);
-          const float fx = (float)(s.x - org.x), fy = (float)(s.y - org.y),
-                      fz = (float)(s.z - org.z), fw = (float)w;
-          buf[2 * lane] = make_ulonglong2(pack2(fx, fx), pack2(fy, fy));
-          buf[2 * lane + 1] = make_ulonglong2(pack2(fz, fz), pack2(fw, fw));
-        }
-        __syncwarp();
-        if (guard) pairs_mixed<NP2, true>(tx, ty, tz, hi, lo, buf, cnt);
-        else pairs_mixed<NP2, false>(tx, ty, tz, hi, lo, buf, cnt);
-        __syncwarp();
+      if (lane < cnt) {
+        const float fx = (float)(s.x - org.x), fy = (float)(s.y - org.y),
+                    fz = (float)(s.z - org.z), fw = (float)w;
+        buf[2 * lane] = make_ulonglong2(pack2(fx, fx), pack2(fy, fy));
+        buf[2 * lane + 1] = make_ulonglong2(pack2(fz, fz), pack2(fw, fw));
       }
+      __syncwarp();
+      c0 += 32;
+      if (c0 >= count) {
+        ++e;
+        c0 = 0;
+        open_entry();
+      }
+      if (e < J.eend && lane < min(32, count - c0))
+        load_entry_source(p, kind, node, base, c0 + lane, s, w);
+      if (guard) pairs_mixed<NS, true>(tx, ty, tz, hi, lo, buf, cnt);
+      else pairs_mixed<NS, false>(tx, ty, tz, hi, lo, buf, cnt);
+      __syncwarp();
     }
 #pragma unroll
     for (int t = 0; t < NS; ++t) sum[t] = (double)hi[t] + (double)lo[t];
@@ -286,25 +356,22 @@ __device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, in
       acc[t] = 0.0;
     }
     double4* buf = (double4*)wbuf;
-    for (int e = J.ebeg; e < J.eend; ++e) {
-      const int ent = p.entries[e];
-      const int kind = ent >> 28, node = ent & 0x0fffffff;
-      const int count = kind == 0 ? p.src_num[node] : p.P;
-      const int base = kind == 0 ? p.src_beg[node] : 0;
+    while (e < J.eend) {
+      const int cnt = min(32, count - c0);
       const bool guard = kind == 0 && J.tkind == 0 && node == J.tnode;
-      for (int c0 = 0; c0 < count; c0 += 32) {
-        const int cnt = min(32, count - c0);
-        if (lane < cnt) {
-          double3 s;
-          double w;
-          load_entry_source(p, kind, node, base, c0 + lane, s, w);
-          buf[lane] = make_double4(s.x, s.y, s.z, w);
-        }
-        __syncwarp();
-        if (guard) pairs_fp64<NS, true>(tx, ty, tz, acc, buf, cnt);
-        else pairs_fp64<NS, false>(tx, ty, tz, acc, buf, cnt);
-        __syncwarp();
+      if (lane < cnt) buf[lane] = make_double4(s.x, s.y, s.z, w);
+      __syncwarp();
+      c0 += 32;
+      if (c0 >= count) {
+        ++e;
+        c0 = 0;
+        open_entry();
       }
+      if (e < J.eend && lane < min(32, count - c0))
+        load_entry_source(p, kind, node, base, c0 + lane, s, w);
+      if (guard) pairs_fp64<NS, true>(tx, ty, tz, acc, buf, cnt);
+      else pairs_fp64<NS, false>(tx, ty, tz, acc, buf, cnt);
+      __syncwarp();
     }
 #pragma unroll
     for (int t = 0; t < NS; ++t) sum[t] = acc[t];
@@ -321,24 +388,28 @@ __device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, in
   }
 }
 
-template <bool kMixed, int kMaxSlots>
-__global__ void __launch_bounds__(32 * kWarpJobsPerBlock, kMixed ? 6 : 4)
-p2p_warp_kernel(P2PParams p, int njobs) {
+// Persistent: each warp takes jobs from *next_job until none are left.  The
+// counter is zeroed on the stream before every launch.
+template <bool kMixed>
+__global__ void __launch_bounds__(32 * kWarpJobsPerBlock, kMixed ? KFMM_P2P_MIXED_MINB : 4)
+p2p_warp_kernel(P2PParams p, int njobs, int* next_job) {
   __shared__ __align__(16) unsigned char smem[kWarpJobsPerBlock][32 * 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int j = blockIdx.x * kWarpJobsPerBlock + wid;
-  if (j >= njobs) return;
-  const P2PJob J = p.jobs[j];
-  const int slots = (J.tcnt + 31) >> 5;
   void* wb = smem[wid];
-  if constexpr (kMixed) {
-    if (slots > 2) warp_job<true, 4>(p, J, lane, wb);
-    else warp_job<true, 2>(p, J, lane, wb);
-  } else {
-    if (slots == 4) warp_job<false, 4>(p, J, lane, wb);
-    else if (slots == 3) warp_job<false, 3>(p, J, lane, wb);
-    else if (slots == 2) warp_job<false, 2>(p, J, lane, wb);
-    else warp_job<false, 1>(p, J, lane, wb);
+  for (;;) {
+    int j = 0;
+    if (lane == 0) j = atomicAdd(next_job, 1);
+    j = __shfl_sync(0xffffffffu, j, 0);
+    if (j >= njobs) return;
+    const P2PJob J = p.jobs[j];
+    switch ((J.tcnt + 31) >> 5) {
+      case 1: warp_job<kMixed, 1>(p, J, lane, wb); break;
+      case 2: warp_job<kMixed, 2>(p, J, lane, wb); break;
+      case 3: warp_job<kMixed, 3>(p, J, lane, wb); break;
+      case 4: warp_job<kMixed, 4>(p, J, lane, wb); break;
+      case 5: warp_job<kMixed, 5>(p, J, lane, wb); break;
+      default: warp_job<kMixed, kMaxSlots>(p, J, lane, wb); break;
+    }
   }
 }
 

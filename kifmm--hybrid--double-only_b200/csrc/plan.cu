@@ -94,6 +94,8 @@ struct kfmm_plan {
   P2PJob *s2m_jobs = nullptr, *nf_jobs = nullptr, *s2l_jobs = nullptr;
   int *s2m_ent = nullptr, *nf_ent = nullptr, *s2l_ent = nullptr;
   int n_s2m = 0, n_nf = 0, n_s2l = 0;
+  int* job_counter = nullptr;  // persistent P2P work counters: S2M, S2L, near field
+  int p2p_grid = 0;            // resident P2P blocks on the device
   std::vector<GemmBatch> up_gemms, down_gemms;
   int *fft_nodes = nullptr, *ifft_nodes = nullptr;
   int n_fft = 0, n_ifft = 0;
@@ -428,7 +430,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_CUDA(cudaMemset(p->spec, 0, p->cplx * (size_t)nn * p->Fpad));
   KF_CUDA(cudaMemset(p->effv, 0, p->cplx * (size_t)nn * p->Fpad));
 
-  const int chunk = 32 * (p->prec == KFMM_MIXED ? kMaxSlotsMixed : kMaxSlotsFP64);
+  const int chunk = 32 * kMaxSlots;
   auto add_chunks = [&](std::vector<P2PJob>& jobs, int tnode, int tkind, int tbeg0, int tcount,
                         int ebeg, int eend, int out0, int mode) {
     for (int c = 0; c < tcount; c += chunk) {
@@ -448,6 +450,22 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     int kind = ent >> 28, node = ent & 0x0fffffff;
     return kind == 0 ? d->src_num[node] : P;
   };
+  // largest first (target slots x sources) for the persistent P2P kernel
+  auto order_jobs = [&](std::vector<P2PJob>& jobs, const std::vector<int>& ent) {
+    std::vector<std::pair<double, int>> key(jobs.size());
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      double ns = 0;
+      for (int k = jobs[j].ebeg; k < jobs[j].eend; ++k) ns += src_count(ent[k]);
+      key[j] = {-ns * ((jobs[j].tcnt + 31) / 32), (int)j};
+    }
+    std::stable_sort(key.begin(), key.end(),
+                     [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+                       return a.first < b.first;
+                     });
+    std::vector<P2PJob> out(jobs.size());
+    for (size_t j = 0; j < jobs.size(); ++j) out[j] = jobs[key[j].second];
+    jobs.swap(out);
+  };
 
   // --- up: S2M jobs + UC2UE GEMM, then M2M per level
   {
@@ -466,6 +484,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       alpha.push_back(std::ldexp(1.0, -d->depth[i]));
       ++slot;
     }
+    order_jobs(jobs, ent);
     p->n_s2m = (int)jobs.size();
     KF_TRY(upload(p, &p->s2m_jobs, jobs));
     KF_TRY(upload(p, &p->s2m_ent, ent));
@@ -581,6 +600,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       add_chunks(jobs, t, 2, 0, P, e0, (int)ent.size(), t * P, 1);
       p->stats.s2l_pairs += (double)P * ns;
     }
+    order_jobs(jobs, ent);
     p->n_s2l = (int)jobs.size();
     KF_TRY(upload(p, &p->s2l_jobs, jobs));
     KF_TRY(upload(p, &p->s2l_ent, ent));
@@ -626,6 +646,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       add_chunks(jobs, t, 0, d->trg_beg[t], d->trg_num[t], e0, (int)ent.size(), d->trg_beg[t], 0);
       p->stats.u_pairs += (double)d->trg_num[t] * ns;
     }
+    order_jobs(jobs, ent);
     p->n_nf = (int)jobs.size();
     KF_TRY(upload(p, &p->nf_jobs, jobs));
     KF_TRY(upload(p, &p->nf_ent, ent));
@@ -638,6 +659,17 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
                                (int)had_smem_bytes<true>()));
 
   if (p->splitk_doubles) KF_TRY(dalloc(p, &p->splitk, p->splitk_doubles));
+  KF_TRY(dalloc(p, &p->job_counter, 3));
+  {
+    int occ = 0;
+    if (p->prec == KFMM_MIXED)
+      KF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p2p_warp_kernel<true>,
+                                                            32 * kWarpJobsPerBlock, 0));
+    else
+      KF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p2p_warp_kernel<false>,
+                                                            32 * kWarpJobsPerBlock, 0));
+    p->p2p_grid = std::max(1, occ) * p->num_sms;
+  }
   p->stats.num_nodes = nn;
   p->stats.P = P;
   p->stats.Q = Q;
@@ -680,13 +712,15 @@ kfmm_status launch_fft(int np, bool mixed, bool forward, int nblocks, const FFTP
   return KFMM_OK;
 }
 
-kfmm_status launch_p2p(const kfmm_plan* p, int njobs, const P2PParams& q, void* stream,
-                       const char* what) {
-  const int blocks = (njobs + kWarpJobsPerBlock - 1) / kWarpJobsPerBlock;
+kfmm_status launch_p2p(const kfmm_plan* p, int which, int njobs, const P2PParams& q,
+                       void* stream, const char* what) {
+  const int blocks = std::min(p->p2p_grid, (njobs + kWarpJobsPerBlock - 1) / kWarpJobsPerBlock);
+  int* counter = p->job_counter + which;
+  KF_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), S(stream)));
   if (p->prec == KFMM_MIXED)
-    p2p_warp_kernel<true, kMaxSlotsMixed><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(q, njobs);
+    p2p_warp_kernel<true><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(q, njobs, counter);
   else
-    p2p_warp_kernel<false, kMaxSlotsFP64><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(q, njobs);
+    p2p_warp_kernel<false><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(q, njobs, counter);
   KF_CHECK_LAUNCH(std::string("p2p kernel (") + what + ")");
   return KFMM_OK;
 }
@@ -804,7 +838,7 @@ kfmm_status kfmm_up_calc(kfmm_plan* p, void* stream) {
     return KFMM_ERR_STATE;
   }
   if (p->n_s2m) {
-    KF_TRY(launch_p2p(p, p->n_s2m, p2p_params(p, p->s2m_jobs, p->s2m_ent, p->chk_up), stream,
+    KF_TRY(launch_p2p(p, 0, p->n_s2m, p2p_params(p, p->s2m_jobs, p->s2m_ent, p->chk_up), stream,
                       "s2m"));
   }
   return launch_gemms(p, p->up_gemms, S(stream));
@@ -843,7 +877,7 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
 kfmm_status kfmm_xlist_calc(kfmm_plan* p, void* stream) {
   if (!p) return KFMM_ERR_INVALID;
   if (p->n_s2l) {
-    KF_TRY(launch_p2p(p, p->n_s2l, p2p_params(p, p->s2l_jobs, p->s2l_ent, p->dchk), stream,
+    KF_TRY(launch_p2p(p, 1, p->n_s2l, p2p_params(p, p->s2l_jobs, p->s2l_ent, p->dchk), stream,
                       "s2l"));
   }
   return KFMM_OK;
@@ -860,7 +894,7 @@ kfmm_status kfmm_ulist_calc(kfmm_plan* p, void* stream) {
     return KFMM_ERR_STATE;
   }
   if (p->n_nf) {
-    KF_TRY(launch_p2p(p, p->n_nf, p2p_params(p, p->nf_jobs, p->nf_ent, p->pot_leaf), stream,
+    KF_TRY(launch_p2p(p, 2, p->n_nf, p2p_params(p, p->nf_jobs, p->nf_ent, p->pot_leaf), stream,
                       "near field"));
   }
   return KFMM_OK;

@@ -7,7 +7,9 @@
 // evaluation on the B200.  It compiles against the reference's headers; the
 // recipe is the fmmd--b200-dropin rule of oracle/Makefile.
 //
-// env: KFMM_MIXED=1 selects the mixed-precision form.
+// env: KFMM_MIXED=1 selects the mixed-precision form; KFMM_DUMP_POT=<file>
+// writes the potentials (original target order, raw doubles) after run(), so
+// tests can compare them per target with the reference's.
 #include <assert.h>
 #include <math.h>
 #include <stdio.h>
@@ -25,6 +27,7 @@
 struct FMMWrapper {
   AllNodes* AN;
   kfmm_plan* plan;
+  int num_trg;
 };
 
 static void fail(const char* what) {
@@ -144,6 +147,7 @@ FMMWrapper_t* preproc(AllNodes* A) {
   kfmm_precision prec = (m && atoi(m) == 1) ? KFMM_MIXED : KFMM_PLAIN_FP64;
   FMMWrapper_t* F = (FMMWrapper_t*)calloc(1, sizeof(FMMWrapper_t));
   F->AN = A;
+  F->num_trg = d.num_trg;
   if (kfmm_plan_create_with_operators(&d, getenv__accuracy(), prec, &ops, &F->plan) != KFMM_OK)
     fail("kfmm_plan_create_with_operators");
   return F;
@@ -155,6 +159,14 @@ int run(FMMWrapper_t* F) {
   if (kfmm_evaluate(F->plan, A->sx_orig, A->sy_orig, A->sz_orig, A->den_orig, A->tx_orig,
                     A->ty_orig, A->tz_orig, A->pot_orig, NULL) != KFMM_OK)
     fail("kfmm_evaluate");
+  if (const char* path = getenv("KFMM_DUMP_POT")) {
+    FILE* f = fopen(path, "wb");
+    if (!f || fwrite(A->pot_orig, sizeof(double), F->num_trg, f) != (size_t)F->num_trg) {
+      fprintf(stderr, "KFMM_DUMP_POT: cannot write %s\n", path);
+      exit(-1);
+    }
+    fclose(f);
+  }
   float ms[6];
   if (kfmm_phase_times(F->plan, ms) != KFMM_OK) fail("kfmm_phase_times");
   long double t_up = ms[0] * 1e-3L, t_v = ms[1] * 1e-3L, t_x = ms[2] * 1e-3L;
