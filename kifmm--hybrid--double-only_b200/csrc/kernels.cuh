@@ -6,8 +6,8 @@
 //   ctr[n]       node centre and radius (cx, cy, cz, r)       double4
 //   uden/dchk/dden[n*P + k]   upward equivalent density, downward check
 //                potential, downward equivalent density      double
-//   spec/effv[fb][n][16]      source / target spectra, frequency-blocked
-//                (see spec_index)                            double2
+//   spec/effv[fb][n][32]      source / target spectra, frequency-blocked
+//                (see spec_index)             double2 or float2 (mixed)
 #pragma once
 
 #include <cuda_runtime.h>
@@ -760,22 +760,16 @@ struct HadamardParams {
   int nn, ngroups, groups_per_block;
   const int* win;      // ngroups x 216 node ids (-1 = absent)
   const int* members;  // ngroups x 8 node ids (-1 = no V list)
-  // 343 x Fpad translation spectra, zero for |delta|_inf <= 1 and f >= F:
-  // double2 (FP64) or float2 (mixed)
-  const void* trans;
+  // 343 x Fpad translation spectra, zero for |delta|_inf <= 1 and f >= F
+  const double2* trans;
   int Fpad;
-  const void* spec;  // blocked layout, double2 or float2
-  void* effv;        // blocked layout, double2 or float2
+  const double2* spec;  // blocked layout
+  double2* effv;        // blocked layout
 };
 
 constexpr int kHadThreads = 256;  // 8 warps, one group per warp, lane = frequency
 constexpr int kHadGroupsInFlight = kHadThreads / 32;
 constexpr int kHadGroupsPerBlock = 32;
-
-template <bool kMixed>
-__host__ __device__ constexpr size_t had_smem_bytes() {
-  return kMixed ? sizeof(float2) * 343 * kFB : 0;
-}
 
 __device__ __forceinline__ void cmac64(double& ar, double& ai, const double2 t, const double2 s) {
   ar = fma(t.x, s.x, ar);
@@ -784,67 +778,20 @@ __device__ __forceinline__ void cmac64(double& ar, double& ai, const double2 t, 
   ai = fma(t.y, s.x, ai);
 }
 
-// acc {re, im} += t * s with packed FP32: t01 = {tr, tr}, t23 = {-ti, ti},
-// s = {sr, si}, sw = {si, sr}.
-__device__ __forceinline__ unsigned long long cmac32x2(unsigned long long acc,
-                                                       unsigned long long t01,
-                                                       unsigned long long t23,
-                                                       unsigned long long s,
-                                                       unsigned long long sw) {
-  asm("fma.rn.f32x2 %0, %1, %2, %0;\n"
-      "fma.rn.f32x2 %0, %3, %4, %0;\n"
-      : "+l"(acc)
-      : "l"(t01), "l"(s), "l"(t23), "l"(sw));
-  return acc;
-}
-
-// packed two-sum: (hi, lo) += b, both halves at once
-__device__ __forceinline__ void two_sum32x2(unsigned long long& hi, unsigned long long& lo,
-                                            unsigned long long b) {
-  asm("{\n"
-      " .reg .b64 s, bp, ap, t1, t2;\n"
-      " add.f32x2 s, %0, %2;\n"
-      " sub.f32x2 bp, s, %0;\n"
-      " sub.f32x2 ap, s, bp;\n"
-      " sub.f32x2 t1, %0, ap;\n"
-      " sub.f32x2 t2, %2, bp;\n"
-      " add.f32x2 %1, %1, t1;\n"
-      " add.f32x2 %1, %1, t2;\n"
-      " mov.b64 %0, s;\n"
-      "}\n"
-      : "+l"(hi), "+l"(lo)
-      : "l"(b));
-}
-
-// One block: one block of 32 frequencies (blockIdx.y) for groups_per_block
-// groups.  Warp = one group, lane = one frequency, all 8 members of the group
-// in registers; every shared or global load of a warp is 32 distinct,
-// contiguous values.  The 343 translation spectra of the frequency block sit
-// in shared memory (zero at the adjacent offsets: every window entry is a
-// plain multiply-add).  The window is walked row by row in x: a row of 6
-// source spectra meets, for each of the 4 (cy, cz) member pairs, one row of 7
-// translation spectra: 12 complex multiply-adds per 7 shared loads; the next
-// row's source spectra are fetched while the current row is multiplied.  The
-// FP32 instance (mixed form) uses packed f32x2 multiply-adds and adds each
-// member's two-row partial sums into a two-sum (hi, lo) pair.
-template <bool kMixed>
+// Plain FP64 form.  One block: one block of 32 frequencies (blockIdx.y) for
+// groups_per_block groups.  Warp = one group, lane = one frequency, all 8
+// members of the group in registers; every load of a warp is 32 distinct,
+// contiguous values.  The translation spectra are read through L1 (the
+// frequency block's FP64 tile, 176 KB, would leave room for one block per
+// SM).  The window is walked row by row in x: a row of 6 source spectra
+// meets, for each of the 4 (cy, cz) member pairs, one row of 7 translation
+// spectra: 12 complex multiply-adds per 7 loads; the next row's source
+// spectra are fetched while the current row is multiplied.
 __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p) {
-  extern __shared__ __align__(16) unsigned char had_dyn[];
   __shared__ int win[kHadGroupsInFlight][216];
   __shared__ int mem[kHadGroupsInFlight][8];
-  using C = typename std::conditional<kMixed, float2, double2>::type;
-  const C* spec = (const C*)p.spec;
-  const C* trans = (const C*)p.trans;
-  C* effv = (C*)p.effv;
   const int fb = blockIdx.y;
   const int f = threadIdx.x & 31, slot = threadIdx.x >> 5;
-  // FP32: the frequency block's translation spectra in shared memory
-  // (343 x 32 x 8 B); FP64 reads them through L1 (the 176 KB tile would
-  // leave room for one block per SM)
-  C* tsm = (C*)had_dyn;
-  if (kMixed)
-    for (int q = threadIdx.x; q < 343 * kFB; q += kHadThreads)
-      tsm[q] = trans[(size_t)(q / kFB) * p.Fpad + fb * kFB + (q % kFB)];
   const int g0 = blockIdx.x * p.groups_per_block;
   const int g1 = min(p.ngroups, g0 + p.groups_per_block);
   const size_t fbase = (size_t)fb * p.nn;
@@ -861,105 +808,213 @@ __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p)
     __syncthreads();
     if (gb + slot >= g1) continue;  // warp-uniform: no group for this warp
     const int* w = win[slot];
-    C nxt[6];
+    double2 nxt[6];
 #pragma unroll
     for (int wx = 0; wx < 6; ++wx) {
       const int sid = w[wx];
-      nxt[wx] = sid >= 0 ? spec[(fbase + sid) * kFB + f] : C{0, 0};
+      nxt[wx] = sid >= 0 ? p.spec[(fbase + sid) * kFB + f] : make_double2(0.0, 0.0);
     }
-    if constexpr (kMixed) {
-      unsigned long long acc[8], hi[8], lo[8];
+    double ar[8], ai[8];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) acc[c] = hi[c] = lo[c] = 0ull;
-      for (int row = 0; row < 36; ++row) {
-        unsigned long long sr[6], sw[6];
+    for (int c = 0; c < 8; ++c) ar[c] = ai[c] = 0.0;
+    for (int row = 0; row < 36; ++row) {
+      double2 srow[6];
+#pragma unroll
+      for (int wx = 0; wx < 6; ++wx) srow[wx] = nxt[wx];
+      if (row + 1 < 36) {
 #pragma unroll
         for (int wx = 0; wx < 6; ++wx) {
-          sr[wx] = pack2(nxt[wx].x, nxt[wx].y);
-          sw[wx] = pack2(nxt[wx].y, nxt[wx].x);
-        }
-        if (row + 1 < 36) {
-#pragma unroll
-          for (int wx = 0; wx < 6; ++wx) {
-            const int sid = w[(row + 1) * 6 + wx];
-            nxt[wx] = sid >= 0 ? spec[(fbase + sid) * kFB + f] : C{0, 0};
-          }
-        }
-        const int wy = row % 6, wz = row / 6;
-#pragma unroll
-        for (int cyz = 0; cyz < 4; ++cyz) {
-          const int cy = cyz >> 1, cz = cyz & 1;
-          const C* trow = tsm + ((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * kFB + f;
-          unsigned long long t01[7], t23[7];
-#pragma unroll
-          for (int k = 0; k < 7; ++k) {
-            const C t = trow[k * kFB];
-            t01[k] = pack2(t.x, t.x);
-            t23[k] = pack2(-t.y, t.y);
-          }
-#pragma unroll
-          for (int wx = 0; wx < 6; ++wx)
-#pragma unroll
-            for (int cx = 0; cx < 2; ++cx) {
-              const int c = cx * 4 + cy * 2 + cz;
-              acc[c] = cmac32x2(acc[c], t01[wx - cx + 1], t23[wx - cx + 1], sr[wx], sw[wx]);
-            }
-        }
-        if (row & 1) {
-#pragma unroll
-          for (int c = 0; c < 8; ++c) {
-            two_sum32x2(hi[c], lo[c], acc[c]);
-            acc[c] = 0ull;
-          }
+          const int sid = w[(row + 1) * 6 + wx];
+          nxt[wx] = sid >= 0 ? p.spec[(fbase + sid) * kFB + f] : make_double2(0.0, 0.0);
         }
       }
+      const int wy = row % 6, wz = row / 6;
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const int m = mem[slot][c];
-        if (m >= 0)
-          effv[(fbase + m) * kFB + f] =
-              make_float2(lo_of(hi[c]) + lo_of(lo[c]), hi_of(hi[c]) + hi_of(lo[c]));
-      }
-    } else {
-      double ar[8], ai[8];
+      for (int cyz = 0; cyz < 4; ++cyz) {
+        const int cy = cyz >> 1, cz = cyz & 1;
+        const double2* trow =
+            p.trans + (size_t)((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * p.Fpad +
+            fb * kFB + f;
+        double2 t[7];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) ar[c] = ai[c] = 0.0;
-      for (int row = 0; row < 36; ++row) {
-        C srow[6];
+        for (int k = 0; k < 7; ++k) t[k] = __ldg(trow + (size_t)k * p.Fpad);
 #pragma unroll
-        for (int wx = 0; wx < 6; ++wx) srow[wx] = nxt[wx];
-        if (row + 1 < 36) {
+        for (int wx = 0; wx < 6; ++wx)
 #pragma unroll
-          for (int wx = 0; wx < 6; ++wx) {
-            const int sid = w[(row + 1) * 6 + wx];
-            nxt[wx] = sid >= 0 ? spec[(fbase + sid) * kFB + f] : C{0, 0};
+          for (int cx = 0; cx < 2; ++cx) {
+            const int c = cx * 4 + cy * 2 + cz;
+            cmac64(ar[c], ai[c], t[wx - cx + 1], srow[wx]);
           }
-        }
-        const int wy = row % 6, wz = row / 6;
-#pragma unroll
-        for (int cyz = 0; cyz < 4; ++cyz) {
-          const int cy = cyz >> 1, cz = cyz & 1;
-          const C* trow =
-              trans + (size_t)((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * p.Fpad +
-              fb * kFB + f;
-          C t[7];
-#pragma unroll
-          for (int k = 0; k < 7; ++k) t[k] = __ldg(trow + (size_t)k * p.Fpad);
-#pragma unroll
-          for (int wx = 0; wx < 6; ++wx)
-#pragma unroll
-            for (int cx = 0; cx < 2; ++cx) {
-              const int c = cx * 4 + cy * 2 + cz;
-              cmac64(ar[c], ai[c], t[wx - cx + 1], srow[wx]);
-            }
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const int m = mem[slot][c];
-        if (m >= 0) effv[(fbase + m) * kFB + f] = make_double2(ar[c], ai[c]);
       }
     }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int m = mem[slot][c];
+      if (m >= 0) p.effv[(fbase + m) * kFB + f] = make_double2(ar[c], ai[c]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-form Hadamard, one CTA per SM.  The translation spectra of one block of
+// 32 frequencies ([fb][343][32] complex FP32, 87,808 B) are brought into
+// shared memory by bulk asynchronous copies (TMA, cp.async.bulk) that
+// complete on an mbarrier.  A complex multiply-add is two packed FP32 FMAs on
+// the translation value as loaded and the source value duplicated:
+//   A += {tr, ti} * {sr, sr},  B += {tr, ti} * {si, si},
+//   re = A.x - B.y,  im = A.y + B.x
+// so a lane reads 8 B of shared memory per 12/7 multiply-adds and spends no
+// instruction on rearranging it.  The products of one z-plane of the window
+// (72 per member) are summed in FP32 and the plane sums accumulated in FP64.
+// Warps are autonomous: each loads its own group's window into its slice of
+// shared memory.
+constexpr int kHad32Threads = 512;
+constexpr int kHad32Warps = kHad32Threads / 32;
+constexpr unsigned kHad32TileBytes = 343u * kFB * 8u;  // 87,808
+constexpr int kHad32Copies = 7;                         // 49 offsets (12,544 B) each
+constexpr long long kMbarSpinLimit = 1ll << 24;          // bounded waits
+
+struct Had32Params {
+  int nn, ngroups, groups_per_block;
+  const int* win;
+  const int* members;
+  const float2* tile;  // [fb][343][32] translation spectra
+  const float2* spec;
+  float2* effv;
+  int* error;  // set to 1 when the tile copy does not complete
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+  for (long long i = 0; i < kMbarSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__global__ void __launch_bounds__(kHad32Threads, 1) hadamard_fp32_kernel(Had32Params p) {
+  extern __shared__ __align__(128) unsigned char had32_dyn[];
+  __shared__ int win[kHad32Warps][216];
+  __shared__ int mem[kHad32Warps][8];
+  __shared__ __align__(8) unsigned long long bar;
+  const unsigned long long* tsm = (const unsigned long long*)had32_dyn;
+  const int fb = blockIdx.y;
+  const int f = threadIdx.x & 31, slot = threadIdx.x >> 5;
+  const unsigned b = smem_addr(&bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b),
+                 "r"(kHad32TileBytes)
+                 : "memory");
+    const unsigned char* src = (const unsigned char*)(p.tile + (size_t)fb * 343 * kFB);
+    constexpr unsigned chunk = kHad32TileBytes / kHad32Copies;
+#pragma unroll 1
+    for (int c = 0; c < kHad32Copies; ++c)
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+          "[%3];\n" ::"r"(smem_addr(had32_dyn + c * chunk)),
+          "l"(src + (size_t)c * chunk), "r"(chunk), "r"(b)
+          : "memory");
+  }
+  // this warp's groups: g0 + slot, g0 + slot + 16, ...
+  const int g0 = blockIdx.x * p.groups_per_block;
+  const int g1 = min(p.ngroups, g0 + p.groups_per_block);
+  const size_t fbase = (size_t)fb * p.nn;
+  const bool ready = mbar_wait_bounded(b, 0);
+  if (!__syncthreads_and(ready)) {
+    if (threadIdx.x == 0) {
+      atomicExch(p.error, 1);
+      mbar_wait_bounded(b, 0);  // let copies still in flight land before exiting
+    }
+    return;
+  }
+  for (int g = g0 + slot; g < g1; g += kHad32Warps) {
+    for (int q = f; q < 216; q += 32) win[slot][q] = p.win[(size_t)g * 216 + q];
+    if (f < 8) mem[slot][f] = p.members[(size_t)g * 8 + f];
+    __syncwarp();
+    const int* w = win[slot];
+    unsigned long long nxt[6];
+#pragma unroll
+    for (int wx = 0; wx < 6; ++wx) {
+      const int sid = w[wx];
+      nxt[wx] = sid >= 0 ? *(const unsigned long long*)&p.spec[(fbase + sid) * kFB + f] : 0ull;
+    }
+    unsigned long long A[8], B[8];
+    double ar[8], ai[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      A[c] = B[c] = 0ull;
+      ar[c] = ai[c] = 0.0;
+    }
+    for (int row = 0; row < 36; ++row) {
+      unsigned long long sr[6], si[6];  // {sr, sr}, {si, si}
+#pragma unroll
+      for (int wx = 0; wx < 6; ++wx) {
+        sr[wx] = pack2(lo_of(nxt[wx]), lo_of(nxt[wx]));
+        si[wx] = pack2(hi_of(nxt[wx]), hi_of(nxt[wx]));
+      }
+      if (row + 1 < 36) {
+#pragma unroll
+        for (int wx = 0; wx < 6; ++wx) {
+          const int sid = w[(row + 1) * 6 + wx];
+          nxt[wx] =
+              sid >= 0 ? *(const unsigned long long*)&p.spec[(fbase + sid) * kFB + f] : 0ull;
+        }
+      }
+      const int wy = row % 6, wz = row / 6;
+#pragma unroll
+      for (int cyz = 0; cyz < 4; ++cyz) {
+        const int cy = cyz >> 1, cz = cyz & 1;
+        const unsigned long long* trow =
+            tsm + ((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * kFB + f;
+        unsigned long long t[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) t[k] = trow[k * kFB];
+#pragma unroll
+        for (int wx = 0; wx < 6; ++wx)
+#pragma unroll
+          for (int cx = 0; cx < 2; ++cx) {
+            const int c = cx * 4 + cy * 2 + cz;
+            const unsigned long long tk = t[wx - cx + 1];
+            asm("fma.rn.f32x2 %0, %2, %3, %0;\n"
+                "fma.rn.f32x2 %1, %2, %4, %1;\n"
+                : "+l"(A[c]), "+l"(B[c])
+                : "l"(tk), "l"(sr[wx]), "l"(si[wx]));
+          }
+      }
+      if (wy == 5) {  // end of a z-plane of the window
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          ar[c] += (double)lo_of(A[c]) - (double)hi_of(B[c]);
+          ai[c] += (double)hi_of(A[c]) + (double)lo_of(B[c]);
+          A[c] = B[c] = 0ull;
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int m = mem[slot][c];
+      if (m >= 0) p.effv[(fbase + m) * kFB + f] = make_float2((float)ar[c], (float)ai[c]);
+    }
+    __syncwarp();
   }
 }
 

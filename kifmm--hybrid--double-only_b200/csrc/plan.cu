@@ -95,6 +95,8 @@ struct kfmm_plan {
   int *s2m_ent = nullptr, *nf_ent = nullptr, *s2l_ent = nullptr;
   int n_s2m = 0, n_nf = 0, n_s2l = 0;
   int* job_counter = nullptr;  // persistent P2P work counters: S2M, S2L, near field
+  int* d_error = nullptr;      // set by kernels whose bounded waits ran out
+  int had32_groups_per_block = 0;
   int p2p_grid = 0;            // resident P2P blocks on the device
   std::vector<GemmBatch> up_gemms, down_gemms;
   int *fft_nodes = nullptr, *ifft_nodes = nullptr;
@@ -356,11 +358,15 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   p->Fpad = (F + kFB - 1) / kFB * kFB;
   p->cplx = p->prec == KFMM_MIXED ? sizeof(float2) : sizeof(double2);
   if (p->prec == KFMM_MIXED) {
-    std::vector<float2> tr((size_t)343 * p->Fpad, make_float2(0.f, 0.f));
+    // [fb][343][32]: one contiguous 87,808-byte tile per block of 32
+    // frequencies (hadamard_fp32_kernel)
+    const int nfb = p->Fpad / kFB;
+    std::vector<float2> tr((size_t)nfb * 343 * kFB, make_float2(0.f, 0.f));
     for (int id = 0; id < 343; ++id)
       for (int f = 0; f < F; ++f)
-        tr[(size_t)id * p->Fpad + f] = make_float2((float)op.ue2dc[2 * ((size_t)id * F + f)],
-                                                   (float)op.ue2dc[2 * ((size_t)id * F + f) + 1]);
+        tr[((size_t)(f / kFB) * 343 + id) * kFB + f % kFB] =
+            make_float2((float)op.ue2dc[2 * ((size_t)id * F + f)],
+                        (float)op.ue2dc[2 * ((size_t)id * F + f) + 1]);
     float2* d = nullptr;
     KF_TRY(upload(p, &d, tr));
     p->d_trans = d;
@@ -652,14 +658,20 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     KF_TRY(upload(p, &p->nf_ent, ent));
   }
 
-  KF_CUDA(cudaFuncSetAttribute(hadamard_kernel<false>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)had_smem_bytes<false>()));
-  KF_CUDA(cudaFuncSetAttribute(hadamard_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)had_smem_bytes<true>()));
+  KF_CUDA(cudaFuncSetAttribute(hadamard_fp32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kHad32TileBytes));
+  {
+    // about 8 waves of one CTA per SM over (group chunks x frequency blocks)
+    const int nfb = p->Fpad / kFB;
+    const int max_chunks = std::max(1, (p->n_groups + kHad32Warps - 1) / kHad32Warps);
+    const int chunks = std::max(1, std::min(max_chunks, (8 * p->num_sms + nfb - 1) / nfb));
+    p->had32_groups_per_block = (p->n_groups + chunks - 1) / chunks;
+  }
 
   if (p->splitk_doubles) KF_TRY(dalloc(p, &p->splitk, p->splitk_doubles));
   KF_TRY(dalloc(p, &p->job_counter, 3));
+  KF_TRY(dalloc(p, &p->d_error, 1));
+  KF_CUDA(cudaMemset(p->d_error, 0, sizeof(int)));
   {
     int occ = 0;
     if (p->prec == KFMM_MIXED)
@@ -856,14 +868,22 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
     KF_TRY(launch_fft(p->np, mixed, true, p->n_fft, f, stream));
   }
   if (p->n_groups) {
-    HadamardParams h{p->nn, p->n_groups, kHadGroupsPerBlock, p->win, p->members, p->d_trans,
-                     p->Fpad, p->spec, p->effv};
-    dim3 grid((p->n_groups + kHadGroupsPerBlock - 1) / kHadGroupsPerBlock, p->Fpad / kFB);
-    if (mixed)
-      hadamard_kernel<true><<<grid, kHadThreads, had_smem_bytes<true>(), S(stream)>>>(h);
-    else
-      hadamard_kernel<false><<<grid, kHadThreads, had_smem_bytes<false>(), S(stream)>>>(h);
-    KF_CHECK_LAUNCH("hadamard_kernel");
+    if (mixed) {
+      const int gpb = p->had32_groups_per_block;
+      Had32Params h{p->nn, p->n_groups, gpb, p->win, p->members,
+                    (const float2*)p->d_trans, (const float2*)p->spec, (float2*)p->effv,
+                    p->d_error};
+      dim3 grid((p->n_groups + gpb - 1) / gpb, p->Fpad / kFB);
+      hadamard_fp32_kernel<<<grid, kHad32Threads, kHad32TileBytes, S(stream)>>>(h);
+      KF_CHECK_LAUNCH("hadamard_fp32_kernel");
+    } else {
+      HadamardParams h{p->nn, p->n_groups, kHadGroupsPerBlock, p->win, p->members,
+                       (const double2*)p->d_trans, p->Fpad, (const double2*)p->spec,
+                       (double2*)p->effv};
+      dim3 grid((p->n_groups + kHadGroupsPerBlock - 1) / kHadGroupsPerBlock, p->Fpad / kFB);
+      hadamard_kernel<<<grid, kHadThreads, 0, S(stream)>>>(h);
+      KF_CHECK_LAUNCH("hadamard_kernel");
+    }
   }
   if (p->n_ifft) {
     f.nodes = p->ifft_nodes;
@@ -907,7 +927,13 @@ kfmm_status kfmm_copy_trg_val(kfmm_plan* p, double* pot_host, void* stream) {
   if (pot_host) {
     KF_CUDA(cudaMemcpyAsync(pot_host, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToHost,
                             S(stream)));
+    int err = 0;
+    KF_CUDA(cudaMemcpyAsync(&err, p->d_error, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
     KF_CUDA(cudaStreamSynchronize(S(stream)));
+    if (err) {
+      set_error("a kernel's bounded wait ran out (V-list translation tile copy)");
+      return KFMM_ERR_CUDA;
+    }
   }
   return KFMM_OK;
 }

@@ -184,3 +184,30 @@ def test_mixed_precision_accuracy(K, oracle_mod, cuda_ok, case):
           f"mixed vs plain {vs_plain:.3e}")
     assert np.all(np.isfinite(mixed))
     assert e_mixed <= 2.0 * e_plain
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [("uniform", 65536, 128, 6, 0), ("ellipsoidSurface", 60000, 40, 4, 0),
+                                  ("ellipseUniformAngles", 20000, 32, 3, 0)], ids=_ids)
+def test_mixed_downward_check_vs_plain(K, cuda_ok, case):
+    """The mixed form's V list (FP32 spectra and products, plane sums in
+    FP64) and S2L (FP32 P2P) against the plain path, on the downward check
+    potentials they produce: per node max|d| / max|plain| <= 2e-5 (FP32
+    rounding of the spectra and terms, ~6e-8 each, summed over up to 189
+    V-list boxes)."""
+    dist, n, ppb, np_, coincide = case
+    pts = K.generate_points(n, dist, coincide, 26)
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], ppb)
+    P, _, _ = K.sizes(np_)
+    nn = tree.desc.num_nodes
+    out = {}
+    for prec in (K.PLAIN_FP64, K.MIXED):
+        plan = K.Plan(tree, np_, prec)
+        plan.evaluate(pts)
+        out[prec] = plan.read(1, nn * P)
+        plan.close()
+    tag = tree.array("tag")
+    nodes = np.where(((tag & 2) != 0) & (np.abs(out[K.PLAIN_FP64].reshape(-1, P)).max(axis=1) > 0))[0]
+    e = _node_err(out[K.MIXED], out[K.PLAIN_FP64], P, nodes)
+    print(f"{_ids(case)}: mixed vs plain downward check potentials {e:.2e} over {len(nodes)} nodes")
+    assert len(nodes) > 0 and e <= 2e-5
