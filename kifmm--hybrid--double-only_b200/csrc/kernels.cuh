@@ -63,15 +63,8 @@ __device__ __forceinline__ double3 surface_point(const double4 c, const double* 
 // Mixed precision P2P (kMixed below): coordinates are taken relative to the
 // target set's own node centre in FP64 and then rounded to FP32, so the FP32
 // differences keep ~1e-7 of the box size; 1/r comes from the FP32 reciprocal
-// square root; terms are summed in blocks of 8 whose sums enter a two-sum
-// (hi, lo) pair; the result is formed in FP64 as (hi + lo) / (4 pi).
-__device__ __forceinline__ void two_sum(float& hi, float& lo, float b) {
-  const float s = hi + b;
-  const float bp = s - hi;
-  const float ap = s - bp;
-  lo += (hi - ap) + (b - bp);
-  hi = s;
-}
+// square root; terms are summed in FP32 over blocks of 16 sources and the
+// block sums in FP64; the result is scaled by 1/(4 pi) in FP64.
 
 // ---------------------------------------------------------------------------
 // Warp-autonomous P2P.  One warp owns one job of up to 32*kMaxSlots targets
@@ -228,18 +221,19 @@ __device__ __forceinline__ float pair_term1(float tx, float ty, float tz, float 
 }
 
 // NS targets per lane: NS / 2 packed pairs, plus one scalar target when NS is
-// odd (the high half of the last packed register is then unused).
+// odd (the high half of the last packed register is then unused).  Terms are
+// summed in FP32 over blocks of 16 sources; the block sums are accumulated in
+// FP64 (acc), which keeps the long sum as accurate as a compensated FP32 sum
+// and leaves the FP32 pipe to the pair terms.
 // buf: per source {x,x},{y,y} then {z,z},{w,w} (two ulonglong2 per source).
 template <int NS, bool kGuard>
 __device__ __forceinline__ void pairs_mixed(const unsigned long long (&tx)[(NS + 1) / 2],
                                             const unsigned long long (&ty)[(NS + 1) / 2],
                                             const unsigned long long (&tz)[(NS + 1) / 2],
-                                            float (&hi)[NS], float (&lo)[NS],
-                                            const ulonglong2* buf, int cnt) {
-  constexpr int NP2 = NS / 2, ODD = NS & 1;
-  int k = 0;
-  while (k < cnt) {
-    const int m = min(8, cnt - k);
+                                            double (&acc)[NS], const ulonglong2* buf, int cnt) {
+  constexpr int NP2 = NS / 2, ODD = NS & 1, kBlock = 16;
+  for (int k = 0; k < cnt; k += kBlock) {
+    const int m = min(kBlock, cnt - k);
     unsigned long long blk[NP2 > 0 ? NP2 : 1];
     float blk1 = 0.f;
 #pragma unroll
@@ -252,20 +246,19 @@ __device__ __forceinline__ void pairs_mixed(const unsigned long long (&tx)[(NS +
         blk1 = pair_term1<kGuard>(lo_of(tx[NP2]), lo_of(ty[NP2]), lo_of(tz[NP2]), lo_of(a.x),
                                   lo_of(a.y), lo_of(b.x), lo_of(b.y), blk1);
     };
-    if (m == 8) {
+    if (m == kBlock) {
       constexpr int kUnroll = NS > 4 ? 2 : 4;  // bounds the live pair temporaries
 #pragma unroll kUnroll
-      for (int u = 0; u < 8; ++u) step(u);
+      for (int u = 0; u < kBlock; ++u) step(u);
     } else {
       for (int u = 0; u < m; ++u) step(u);
     }
 #pragma unroll
     for (int t = 0; t < NP2; ++t) {
-      two_sum(hi[2 * t], lo[2 * t], lo_of(blk[t]));
-      two_sum(hi[2 * t + 1], lo[2 * t + 1], hi_of(blk[t]));
+      acc[2 * t] += (double)lo_of(blk[t]);
+      acc[2 * t + 1] += (double)hi_of(blk[t]);
     }
-    if (ODD) two_sum(hi[NS - 1], lo[NS - 1], blk1);
-    k += m;
+    if (ODD) acc[NS - 1] += (double)blk1;
   }
 }
 
@@ -318,9 +311,9 @@ __device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, in
       ty[t] = pack2((float)(q[2 * t][1] - org.y), (float)(q[u][1] - org.y));
       tz[t] = pack2((float)(q[2 * t][2] - org.z), (float)(q[u][2] - org.z));
     }
-    float hi[NS], lo[NS];
+    double acc[NS];
 #pragma unroll
-    for (int t = 0; t < NS; ++t) hi[t] = lo[t] = 0.f;
+    for (int t = 0; t < NS; ++t) acc[t] = 0.0;
     ulonglong2* buf = (ulonglong2*)wbuf;
     while (e < J.eend) {
       const int cnt = min(32, count - c0);
@@ -340,12 +333,12 @@ __device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, in
       }
       if (e < J.eend && lane < min(32, count - c0))
         load_entry_source(p, kind, node, base, c0 + lane, s, w);
-      if (guard) pairs_mixed<NS, true>(tx, ty, tz, hi, lo, buf, cnt);
-      else pairs_mixed<NS, false>(tx, ty, tz, hi, lo, buf, cnt);
+      if (guard) pairs_mixed<NS, true>(tx, ty, tz, acc, buf, cnt);
+      else pairs_mixed<NS, false>(tx, ty, tz, acc, buf, cnt);
       __syncwarp();
     }
 #pragma unroll
-    for (int t = 0; t < NS; ++t) sum[t] = (double)hi[t] + (double)lo[t];
+    for (int t = 0; t < NS; ++t) sum[t] = acc[t];
   } else {
     double tx[NS], ty[NS], tz[NS], acc[NS];
 #pragma unroll
