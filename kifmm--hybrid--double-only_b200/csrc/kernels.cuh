@@ -562,6 +562,7 @@ __host__ __device__ __forceinline__ size_t spec_index(int f, int node, int nn) {
 
 struct FFTParams {
   int np, P, F, nn;
+  int nboxes;           // entries of nodes
   const int* nodes;     // nodes to transform
   const int* depth;
   const int* surf_idx;  // np^3 -> surface index or -1, index (i*np + j)*np + k
@@ -577,37 +578,58 @@ struct FFTParams {
 constexpr int kFFTThreads = 128;
 constexpr int kMaxNP = 8;
 
-// Pruned 3-D transforms of one box per block, compiled per NP so every loop
-// over the np^3 surface block unrolls and every twiddle index is a constant
-// (the twiddle loads are then warp-wide broadcasts).  Each pass gives one
-// thread one line of the grid: the x pass a (z, y) row, the y pass a (z, kx)
-// column, the z pass a (ky, kx) column, and each thread produces all outputs
-// of its line from the <= np non-zero inputs.
+// Boxes per block: as many as fit in ~44 KB of static shared memory (at most
+// 3), so that every pass keeps most of the block's threads busy.
+template <int NP>
+__host__ __device__ constexpr int fft_boxes_per_block() {
+  constexpr int N = 2 * NP, NK = NP + 1;
+  constexpr int fwd = NP * NP * NP * 8 + NP * NP * NK * 16 + NP * N * NK * 16;
+  constexpr int b = 44000 / fwd;
+  return b < 1 ? 1 : (b > 3 ? 3 : b);
+}
+
+// Pruned 3-D transforms, compiled per NP so every loop over the np^3 surface
+// block unrolls and every twiddle index is a constant (the twiddle loads are
+// then warp-wide broadcasts).  A block transforms fft_boxes_per_block<NP>()
+// boxes.  Each pass gives one thread one line of one box's grid: the x pass a
+// (z, y) row, the y pass a (z, kx) column, the z pass a (ky, kx) column, and
+// each thread produces all outputs of its line from the <= np non-zero
+// inputs.
 template <int NP, class C>
 __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
-  constexpr int N = 2 * NP, H = NP / 2, NK = NP + 1;
-  __shared__ double den[NP * NP * NP];
-  __shared__ double2 X[NP * NP * NK];
-  __shared__ double2 Y[NP * N * NK];
+  constexpr int N = 2 * NP, H = NP / 2, NK = NP + 1, B = fft_boxes_per_block<NP>();
+  __shared__ double den[B][NP * NP * NP];
+  __shared__ double2 X[B][NP * NP * NK];
+  __shared__ double2 Y[B][NP * N * NK];
   __shared__ double cs[N], sn[N];
-  const int node = p.nodes[blockIdx.x];
-  const double scale = ldexp(1.0, p.depth[node]);
+  __shared__ int node_s[B];
+  __shared__ double scale_s[B];
   const int tid = threadIdx.x;
+  const int b0 = blockIdx.x * B;
   if (tid < N) {
     cs[tid] = p.cs[tid];
     sn[tid] = p.sn[tid];
   }
-  for (int q = tid; q < NP * NP * NP; q += kFFTThreads) {
-    const int sidx = p.surf_idx[q];
-    den[q] = sidx >= 0 ? p.pln[(size_t)node * p.P + sidx] * scale : 0.0;
+  if (tid < B) {
+    const int node = b0 + tid < p.nboxes ? p.nodes[b0 + tid] : -1;
+    node_s[tid] = node;
+    scale_s[tid] = node >= 0 ? ldexp(1.0, p.depth[node]) : 0.0;
+  }
+  __syncthreads();
+  for (int q = tid; q < B * NP * NP * NP; q += kFFTThreads) {
+    const int bb = q / (NP * NP * NP), r = q % (NP * NP * NP);
+    const int node = node_s[bb];
+    const int sidx = p.surf_idx[r];
+    den[bb][r] = (node >= 0 && sidx >= 0) ? p.pln[(size_t)node * p.P + sidx] * scale_s[bb] : 0.0;
   }
   __syncthreads();
   // x: row (k = z, j = y), outputs kx
-  for (int t = tid; t < NP * NP; t += kFFTThreads) {
+  for (int q = tid; q < B * NP * NP; q += kFFTThreads) {
+    const int bb = q / (NP * NP), t = q % (NP * NP);
     const int k = t / NP, j = t % NP;
     double v[NP];
 #pragma unroll
-    for (int i = 0; i < NP; ++i) v[i] = den[(i * NP + j) * NP + k];
+    for (int i = 0; i < NP; ++i) v[i] = den[bb][(i * NP + j) * NP + k];
 #pragma unroll
     for (int kx = 0; kx < NK; ++kx) {
       double ar = 0, ai = 0;
@@ -617,16 +639,17 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
         ar = fma(v[i], cs[m], ar);
         ai = fma(-v[i], sn[m], ai);
       }
-      X[(k * NP + j) * NK + kx] = make_double2(ar, ai);
+      X[bb][(k * NP + j) * NK + kx] = make_double2(ar, ai);
     }
   }
   __syncthreads();
   // y: column (k, kx), outputs ky
-  for (int t = tid; t < NP * NK; t += kFFTThreads) {
+  for (int q = tid; q < B * NP * NK; q += kFFTThreads) {
+    const int bb = q / (NP * NK), t = q % (NP * NK);
     const int k = t / NK, kx = t % NK;
     double2 v[NP];
 #pragma unroll
-    for (int j = 0; j < NP; ++j) v[j] = X[(k * NP + j) * NK + kx];
+    for (int j = 0; j < NP; ++j) v[j] = X[bb][(k * NP + j) * NK + kx];
 #pragma unroll
     for (int ky = 0; ky < N; ++ky) {
       double ar = 0, ai = 0;
@@ -636,17 +659,20 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
         ar = fma(v[j].x, cs[m], fma(v[j].y, sn[m], ar));
         ai = fma(v[j].y, cs[m], fma(-v[j].x, sn[m], ai));
       }
-      Y[(k * N + ky) * NK + kx] = make_double2(ar, ai);
+      Y[bb][(k * N + ky) * NK + kx] = make_double2(ar, ai);
     }
   }
   __syncthreads();
   // z: column (ky, kx), outputs kz -> spectrum
   C* out = (C*)p.specout;
-  for (int t = tid; t < N * NK; t += kFFTThreads) {
+  for (int q = tid; q < B * N * NK; q += kFFTThreads) {
+    const int bb = q / (N * NK), t = q % (N * NK);
+    const int node = node_s[bb];
+    if (node < 0) continue;
     const int ky = t / NK, kx = t % NK;
     double2 v[NP];
 #pragma unroll
-    for (int k = 0; k < NP; ++k) v[k] = Y[(k * N + ky) * NK + kx];
+    for (int k = 0; k < NP; ++k) v[k] = Y[bb][(k * N + ky) * NK + kx];
 #pragma unroll
     for (int kz = 0; kz < N; ++kz) {
       double ar = 0, ai = 0;
@@ -668,22 +694,27 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
 // (omp.cc:482-533, trans.cc:383-418).  Writes plnout[node*P + s].
 template <int NP, class C>
 __global__ void __launch_bounds__(kFFTThreads) ifft_trg_np_kernel(FFTParams p) {
-  constexpr int N = 2 * NP, H = NP / 2, NK = NP + 1;
-  __shared__ double2 Z[NP * N * NK];
-  __shared__ double2 W[NP * NP * NK];
+  constexpr int N = 2 * NP, H = NP / 2, NK = NP + 1, B = fft_boxes_per_block<NP>();
+  __shared__ double2 Z[B][NP * N * NK];
+  __shared__ double2 W[B][NP * NP * NK];
   __shared__ double cs[N], sn[N];
-  const int node = p.nodes[blockIdx.x];
+  __shared__ int node_s[B];
   const int tid = threadIdx.x;
+  const int b0 = blockIdx.x * B;
   if (tid < N) {
     cs[tid] = p.cs[tid];
     sn[tid] = p.sn[tid];
   }
+  if (tid < B) node_s[tid] = b0 + tid < p.nboxes ? p.nodes[b0 + tid] : -1;
   __syncthreads();
   // z inverse: column (ky, kx), outputs z in the surface block; every
   // spectrum entry is read exactly once, straight from global memory
   // (consecutive threads, consecutive entries)
   const C* in = (const C*)p.specin;
-  for (int t = tid; t < N * NK; t += kFFTThreads) {
+  for (int q = tid; q < B * N * NK; q += kFFTThreads) {
+    const int bb = q / (N * NK), t = q % (N * NK);
+    const int node = node_s[bb];
+    if (node < 0) continue;
     const int ky = t / NK, kx = t % NK;
     double2 acc[NP];
 #pragma unroll
@@ -700,18 +731,20 @@ __global__ void __launch_bounds__(kFFTThreads) ifft_trg_np_kernel(FFTParams p) {
       }
     }
 #pragma unroll
-    for (int k = 0; k < NP; ++k) Z[(k * N + ky) * NK + kx] = acc[k];
+    for (int k = 0; k < NP; ++k) Z[bb][(k * N + ky) * NK + kx] = acc[k];
   }
   __syncthreads();
   // y inverse: column (k, kx), outputs y in the surface block
-  for (int t = tid; t < NP * NK; t += kFFTThreads) {
+  for (int q = tid; q < B * NP * NK; q += kFFTThreads) {
+    const int bb = q / (NP * NK), t = q % (NP * NK);
+    if (node_s[bb] < 0) continue;
     const int k = t / NK, kx = t % NK;
     double2 acc[NP];
 #pragma unroll
     for (int j = 0; j < NP; ++j) acc[j] = make_double2(0.0, 0.0);
 #pragma unroll
     for (int ky = 0; ky < N; ++ky) {
-      const double2 v = Z[(k * N + ky) * NK + kx];
+      const double2 v = Z[bb][(k * N + ky) * NK + kx];
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
         const int m = (ky * (j + H)) % N;
@@ -720,15 +753,18 @@ __global__ void __launch_bounds__(kFFTThreads) ifft_trg_np_kernel(FFTParams p) {
       }
     }
 #pragma unroll
-    for (int j = 0; j < NP; ++j) W[(k * NP + j) * NK + kx] = acc[j];
+    for (int j = 0; j < NP; ++j) W[bb][(k * NP + j) * NK + kx] = acc[j];
   }
   __syncthreads();
   // x: Hermitian half -> real, at the surface points only
   constexpr double inv_g = 1.0 / (double)(N * N * N);
   constexpr int P = NP * NP * NP - (NP - 2) * (NP - 2) * (NP - 2);
-  for (int s = tid; s < P; s += kFFTThreads) {
+  for (int q = tid; q < B * P; q += kFFTThreads) {
+    const int bb = q / P, s = q % P;
+    const int node = node_s[bb];
+    if (node < 0) continue;
     const int i = p.surf_ijk[3 * s], j = p.surf_ijk[3 * s + 1], k = p.surf_ijk[3 * s + 2];
-    const double2* w = &W[(k * NP + j) * NK];
+    const double2* w = &W[bb][(k * NP + j) * NK];
     const int x = i + H;
     double acc = w[0].x + ((x & 1) ? -w[NP].x : w[NP].x);
     int m = 0;

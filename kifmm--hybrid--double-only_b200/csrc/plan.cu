@@ -699,7 +699,10 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
 inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
 template <int NP>
-void fft_launch_np(bool mixed, bool forward, int nblocks, const FFTParams& f, cudaStream_t st) {
+void fft_launch_np(bool mixed, bool forward, int nboxes, FFTParams f, cudaStream_t st) {
+  constexpr int B = fft_boxes_per_block<NP>();
+  const int nblocks = (nboxes + B - 1) / B;
+  f.nboxes = nboxes;
   if (forward) {
     if (mixed) fft_src_np_kernel<NP, float2><<<nblocks, kFFTThreads, 0, st>>>(f);
     else fft_src_np_kernel<NP, double2><<<nblocks, kFFTThreads, 0, st>>>(f);
@@ -709,15 +712,15 @@ void fft_launch_np(bool mixed, bool forward, int nblocks, const FFTParams& f, cu
   }
 }
 
-kfmm_status launch_fft(int np, bool mixed, bool forward, int nblocks, const FFTParams& f,
+kfmm_status launch_fft(int np, bool mixed, bool forward, int nboxes, const FFTParams& f,
                        void* stream) {
   switch (np) {
-    case 3: fft_launch_np<3>(mixed, forward, nblocks, f, S(stream)); break;
-    case 4: fft_launch_np<4>(mixed, forward, nblocks, f, S(stream)); break;
-    case 5: fft_launch_np<5>(mixed, forward, nblocks, f, S(stream)); break;
-    case 6: fft_launch_np<6>(mixed, forward, nblocks, f, S(stream)); break;
-    case 7: fft_launch_np<7>(mixed, forward, nblocks, f, S(stream)); break;
-    case 8: fft_launch_np<8>(mixed, forward, nblocks, f, S(stream)); break;
+    case 3: fft_launch_np<3>(mixed, forward, nboxes, f, S(stream)); break;
+    case 4: fft_launch_np<4>(mixed, forward, nboxes, f, S(stream)); break;
+    case 5: fft_launch_np<5>(mixed, forward, nboxes, f, S(stream)); break;
+    case 6: fft_launch_np<6>(mixed, forward, nboxes, f, S(stream)); break;
+    case 7: fft_launch_np<7>(mixed, forward, nboxes, f, S(stream)); break;
+    case 8: fft_launch_np<8>(mixed, forward, nboxes, f, S(stream)); break;
     default: set_error("launch_fft: NP out of range"); return KFMM_ERR_UNSUPPORTED;
   }
   KF_CHECK_LAUNCH(forward ? "fft_src_np_kernel" : "ifft_trg_np_kernel");
