@@ -19,6 +19,10 @@ namespace kfmm {
 
 constexpr double kOOFP = 1.0 / (4.0 * 3.14159265358979323846);
 
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
 // ---------------------------------------------------------------------------
 // P2P engine.  A job evaluates one set of targets against a list of source
 // sets ("entries").  Targets: real points of a leaf (kind 0) or the UC (1) /
@@ -436,24 +440,41 @@ __device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, doubl
 
 // A block computes rows [m0, m0 + mrows) of C (mrows <= 160, a multiple of 8)
 // for kGemmBN columns.  8 warps = 4 (rows) x 2 (columns); each warp owns 5 x 4
-// m8n8 tiles, i.e. 20 DMMA per 4-deep k step for 9 shared loads.  The next
-// 16-deep slice of A and B is fetched into registers while the current one
-// is multiplied from shared memory.
+// m8n8 tiles, i.e. 20 DMMA per 4-deep k step for 9 shared loads.  16-deep
+// slices of A and B stream into a 3-stage shared-memory ring by asynchronous
+// 16-byte copies (cp.async, zero-filled outside the matrices), so no
+// registers hold data in flight and two blocks fit on an SM.  Requires M, K
+// and every column offset even (16-byte aligned pairs of doubles); the host
+// checks this when it builds a batch.
 constexpr int kGemmRows = 160, kGemmBN = 64, kGemmBK = 16, kGemmThreads = 256;
-constexpr int kGemmAPT = kGemmRows * kGemmBK / kGemmThreads;  // A elements per thread per slice
-constexpr int kGemmBPT = kGemmBN * kGemmBK / kGemmThreads;    // B elements per thread per slice
+constexpr int kGemmStages = 3;
+constexpr int kGemmAStride = kGemmRows + 8;  // doubles; 8 and 4 (mod 16): every bank pair
+constexpr int kGemmBStride = kGemmBK + 4;    // hit exactly twice by a warp's fragment reads
+constexpr int kGemmStageDoubles = kGemmBK * kGemmAStride + kGemmBN * kGemmBStride;
+constexpr size_t kGemmSmemBytes = sizeof(double) * kGemmStages * kGemmStageDoubles;
 
-__global__ void __launch_bounds__(kGemmThreads, 1) gemm_fp64_dmma_kernel(GemmArgs g, int mrows) {
-  // strides = 8 and 4 (mod 16) doubles: the fragment reads of a warp then hit
-  // every bank pair exactly twice (the minimum for 32 doubles)
-  __shared__ double As[kGemmBK][kGemmRows + 8];
-  __shared__ double Bs[kGemmBN][kGemmBK + 4];
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_addr(smem)),
+               "l"(gmem), "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 2) gemm_fp64_dmma_kernel(GemmArgs g, int mrows) {
+  extern __shared__ __align__(16) double gsm[];
   __shared__ int boff_s[kGemmBN];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
   const int m0 = blockIdx.x * mrows, n0 = blockIdx.y * kGemmBN;
   const int mend = min(g.M, m0 + mrows);
   const int kb = blockIdx.z * g.ksplit, ke = min(g.K, kb + g.ksplit);
+  const int nslices = ke > kb ? (ke - kb + kGemmBK - 1) / kGemmBK : 0;
   if (tid < kGemmBN) boff_s[tid] = (n0 + tid < g.ncol) ? g.boff[n0 + tid] : -1;
   double acc[5][4][2];
 #pragma unroll
@@ -461,52 +482,55 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_fp64_dmma_kernel(GemmArg
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   __syncthreads();
-  double ra[kGemmAPT], rb[kGemmBPT];
-  auto fetch = [&](int k0) {
+  auto issue = [&](int s) {
+    double* As = gsm + (s % kGemmStages) * kGemmStageDoubles;
+    double* Bs = As + kGemmBK * kGemmAStride;
+    const int k0 = kb + s * kGemmBK;
 #pragma unroll
-    for (int r = 0; r < kGemmAPT; ++r) {
-      const int idx = tid + r * kGemmThreads;
-      const int m = idx % kGemmRows, k = idx / kGemmRows;
+    for (int r = 0; r < kGemmRows * kGemmBK / 2 / kGemmThreads; ++r) {
+      const int q = tid + r * kGemmThreads;
+      const int k = q / (kGemmRows / 2), m = 2 * (q % (kGemmRows / 2));
       const int gm = m0 + m, gk = k0 + k;
-      ra[r] = (gm < mend && gk < ke) ? g.A[(size_t)gk * g.M + gm] : 0.0;
+      const bool ok = gm < mend && gk < ke;
+      cp_async16(As + k * kGemmAStride + m, ok ? g.A + (size_t)gk * g.M + gm : g.A, ok);
     }
 #pragma unroll
-    for (int r = 0; r < kGemmBPT; ++r) {
-      const int idx = tid + r * kGemmThreads;
-      const int k = idx % kGemmBK, n = idx / kGemmBK;
+    for (int r = 0; r < kGemmBN * kGemmBK / 2 / kGemmThreads; ++r) {
+      const int q = tid + r * kGemmThreads;
+      const int n = q / (kGemmBK / 2), k = 2 * (q % (kGemmBK / 2));
       const int gk = k0 + k, bo = boff_s[n];
-      rb[r] = (bo >= 0 && gk < ke) ? g.B[(size_t)bo + gk] : 0.0;
+      const bool ok = bo >= 0 && gk < ke;
+      cp_async16(Bs + n * kGemmBStride + k, ok ? g.B + (size_t)bo + gk : g.B, ok);
     }
   };
-  fetch(kb);
-  for (int k0 = kb; k0 < ke; k0 += kGemmBK) {
 #pragma unroll
-    for (int r = 0; r < kGemmAPT; ++r) {
-      const int idx = tid + r * kGemmThreads;
-      As[idx / kGemmRows][idx % kGemmRows] = ra[r];
-    }
-#pragma unroll
-    for (int r = 0; r < kGemmBPT; ++r) {
-      const int idx = tid + r * kGemmThreads;
-      Bs[idx / kGemmBK][idx % kGemmBK] = rb[r];
-    }
+  for (int s = 0; s < kGemmStages - 1; ++s) {
+    if (s < nslices) issue(s);
+    cp_async_commit();
+  }
+  for (int s = 0; s < nslices; ++s) {
+    cp_async_wait<kGemmStages - 2>();
     __syncthreads();
-    if (k0 + kGemmBK < ke) fetch(k0 + kGemmBK);
+    if (s + kGemmStages - 1 < nslices) issue(s + kGemmStages - 1);
+    cp_async_commit();
+    const double* As = gsm + (s % kGemmStages) * kGemmStageDoubles;
+    const double* Bs = As + kGemmBK * kGemmAStride;
 #pragma unroll
     for (int kk = 0; kk < kGemmBK; kk += 4) {
       double af[5], bf[4];
 #pragma unroll
       for (int mi = 0; mi < 5; ++mi)
-        af[mi] = As[kk + (lane & 3)][wm * 40 + mi * 8 + (lane >> 2)];
+        af[mi] = As[(kk + (lane & 3)) * kGemmAStride + wm * 40 + mi * 8 + (lane >> 2)];
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) bf[ni] = Bs[wn * 32 + ni * 8 + (lane >> 2)][kk + (lane & 3)];
+      for (int ni = 0; ni < 4; ++ni)
+        bf[ni] = Bs[(wn * 32 + ni * 8 + (lane >> 2)) * kGemmBStride + kk + (lane & 3)];
 #pragma unroll
       for (int mi = 0; mi < 5; ++mi)
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) dmma_884(acc[mi][ni][0], acc[mi][ni][1], af[mi], bf[ni]);
     }
-    __syncthreads();
   }
+  cp_async_wait<0>();
 #pragma unroll
   for (int mi = 0; mi < 5; ++mi)
 #pragma unroll
@@ -912,10 +936,6 @@ struct Had32Params {
   float2* effv;
   int* error;  // set to 1 when the tile copy does not complete
 };
-
-__device__ __forceinline__ unsigned smem_addr(const void* p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
 
 __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
   unsigned ok;

@@ -148,6 +148,13 @@ kfmm_status add_gemm(kfmm_plan* p, std::vector<GemmBatch>& out, const double* A,
                      const std::vector<int>& coff, const std::vector<double>* alpha,
                      double alpha_const, int accumulate) {
   if (boff.empty()) return KFMM_OK;
+  // the GEMM kernel copies aligned pairs of doubles
+  bool even = M % 2 == 0 && K % 2 == 0;
+  for (int o : boff) even = even && o % 2 == 0;
+  if (!even) {
+    set_error("add_gemm: operator sizes and column offsets must be even");
+    return KFMM_ERR_UNSUPPORTED;
+  }
   GemmBatch g{};
   g.A = A;
   g.M = M;
@@ -182,7 +189,7 @@ kfmm_status launch_gemms(const kfmm_plan* p, const std::vector<GemmBatch>& gs, c
     GemmArgs a{b.A, b.M, b.K, b.ksplit, b.nsplit > 1 ? p->splitk : nullptr, b.B, b.boff, b.C,
                b.coff, b.alpha, b.alpha_const, b.ncol, b.accumulate};
     dim3 grid(b.chunks, (b.ncol + kGemmBN - 1) / kGemmBN, b.nsplit);
-    gemm_fp64_dmma_kernel<<<grid, kGemmThreads, 0, st>>>(a, b.mrows);
+    gemm_fp64_dmma_kernel<<<grid, kGemmThreads, kGemmSmemBytes, st>>>(a, b.mrows);
     KF_CHECK_LAUNCH("gemm_fp64_dmma_kernel");
     if (b.nsplit > 1) {
       const size_t total = (size_t)b.ncol * b.M;
@@ -658,6 +665,8 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     KF_TRY(upload(p, &p->nf_ent, ent));
   }
 
+  KF_CUDA(cudaFuncSetAttribute(gemm_fp64_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kGemmSmemBytes));
   KF_CUDA(cudaFuncSetAttribute(hadamard_fp32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kHad32TileBytes));
   {
