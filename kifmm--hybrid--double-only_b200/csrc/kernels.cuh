@@ -954,15 +954,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
   return false;
 }
 
-__global__ void __launch_bounds__(kHad32Threads, 1) hadamard_fp32_kernel(Had32Params p) {
-  extern __shared__ __align__(128) unsigned char had32_dyn[];
-  __shared__ int win[kHad32Warps][216];
-  __shared__ int mem[kHad32Warps][8];
-  __shared__ __align__(8) unsigned long long bar;
-  const unsigned long long* tsm = (const unsigned long long*)had32_dyn;
-  const int fb = blockIdx.y;
-  const int f = threadIdx.x & 31, slot = threadIdx.x >> 5;
-  const unsigned b = smem_addr(&bar);
+// Bulk-copies the translation tile of frequency block fb into dst (one
+// thread issues, all wait on the mbarrier with a bounded spin).  Returns false
+// in every thread of the block, after setting *error, if the copy did not
+// complete.
+__device__ __forceinline__ bool had32_load_tile(const float2* tile, int fb, unsigned char* dst,
+                                                unsigned long long* bar, int* error) {
+  const unsigned b = smem_addr(bar);
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -973,28 +971,39 @@ __global__ void __launch_bounds__(kHad32Threads, 1) hadamard_fp32_kernel(Had32Pa
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b),
                  "r"(kHad32TileBytes)
                  : "memory");
-    const unsigned char* src = (const unsigned char*)(p.tile + (size_t)fb * 343 * kFB);
+    const unsigned char* src = (const unsigned char*)(tile + (size_t)fb * 343 * kFB);
     constexpr unsigned chunk = kHad32TileBytes / kHad32Copies;
 #pragma unroll 1
     for (int c = 0; c < kHad32Copies; ++c)
       asm volatile(
           "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-          "[%3];\n" ::"r"(smem_addr(had32_dyn + c * chunk)),
+          "[%3];\n" ::"r"(smem_addr(dst + c * chunk)),
           "l"(src + (size_t)c * chunk), "r"(chunk), "r"(b)
           : "memory");
   }
-  // this warp's groups: g0 + slot, g0 + slot + 16, ...
-  const int g0 = blockIdx.x * p.groups_per_block;
-  const int g1 = min(p.ngroups, g0 + p.groups_per_block);
-  const size_t fbase = (size_t)fb * p.nn;
   const bool ready = mbar_wait_bounded(b, 0);
   if (!__syncthreads_and(ready)) {
     if (threadIdx.x == 0) {
-      atomicExch(p.error, 1);
+      atomicExch(error, 1);
       mbar_wait_bounded(b, 0);  // let copies still in flight land before exiting
     }
-    return;
+    return false;
   }
+  return true;
+}
+
+__global__ void __launch_bounds__(kHad32Threads, 1) hadamard_fp32_kernel(Had32Params p) {
+  extern __shared__ __align__(128) unsigned char had32_dyn[];
+  __shared__ int win[kHad32Warps][216];
+  __shared__ int mem[kHad32Warps][8];
+  __shared__ __align__(8) unsigned long long bar;
+  const unsigned long long* tsm = (const unsigned long long*)had32_dyn;
+  const int fb = blockIdx.y;
+  const int f = threadIdx.x & 31, slot = threadIdx.x >> 5;
+  const int g0 = blockIdx.x * p.groups_per_block;
+  const int g1 = min(p.ngroups, g0 + p.groups_per_block);
+  const size_t fbase = (size_t)fb * p.nn;
+  if (!had32_load_tile(p.tile, fb, had32_dyn, &bar, p.error)) return;
   for (int g = g0 + slot; g < g1; g += kHad32Warps) {
     for (int q = f; q < 216; q += 32) win[slot][q] = p.win[(size_t)g * 216 + q];
     if (f < 8) mem[slot][f] = p.members[(size_t)g * 8 + f];
@@ -1062,6 +1071,115 @@ __global__ void __launch_bounds__(kHad32Threads, 1) hadamard_fp32_kernel(Had32Pa
     for (int c = 0; c < 8; ++c) {
       const int m = mem[slot][c];
       if (m >= 0) p.effv[(fbase + m) * kFB + f] = make_float2((float)ar[c], (float)ai[c]);
+    }
+    __syncwarp();
+  }
+}
+
+// Pairs of sibling groups whose parents are x-neighbours (parent x even and
+// x + 1) share one 8 x 6 x 6 window: a row of 8 source spectra meets each
+// row of 7 translation values for both groups, 24 multiply-adds per 7 shared
+// loads, which halves the shared-memory traffic per multiply-add.  The 16
+// members' FP32 sums are flushed at the end of every z-plane into FP64 sums
+// kept in the warp's slice of shared memory.  12 warps per CTA (up to 168 registers a
+// thread).
+constexpr int kHadPairThreads = 384;
+constexpr int kHadPairWarps = kHadPairThreads / 32;
+constexpr size_t kHadPairSumBytes = sizeof(double) * kHadPairWarps * 16 * 2 * 32;
+constexpr size_t kHadPairSmemBytes = kHad32TileBytes + kHadPairSumBytes;
+
+struct HadPairParams {
+  int nn, npairs, pairs_per_block;
+  const int* win;      // npairs x 288: x8 + 8 * (wy + 6 * wz), -1 = absent
+  const int* members;  // npairs x 16: group 0 members, then group 1
+  const float2* tile;
+  const float2* spec;
+  float2* effv;
+  int* error;
+};
+
+__global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(HadPairParams p) {
+  extern __shared__ __align__(128) unsigned char had32_dyn[];
+  __shared__ int win[kHadPairWarps][288];
+  __shared__ int mem[kHadPairWarps][16];
+  __shared__ __align__(8) unsigned long long bar;
+  const unsigned long long* tsm = (const unsigned long long*)had32_dyn;
+  const int fb = blockIdx.y;
+  const int f = threadIdx.x & 31, slot = threadIdx.x >> 5;
+  double* sums = (double*)(had32_dyn + kHad32TileBytes) + (size_t)slot * 16 * 2 * 32 + f;
+  const int g0 = blockIdx.x * p.pairs_per_block;
+  const int g1 = min(p.npairs, g0 + p.pairs_per_block);
+  const size_t fbase = (size_t)fb * p.nn;
+  if (!had32_load_tile(p.tile, fb, had32_dyn, &bar, p.error)) return;
+  for (int g = g0 + slot; g < g1; g += kHadPairWarps) {
+    for (int q = f; q < 288; q += 32) win[slot][q] = p.win[(size_t)g * 288 + q];
+    if (f < 16) mem[slot][f] = p.members[(size_t)g * 16 + f];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) sums[c * 32] = 0.0;
+    __syncwarp();
+    const int* w = win[slot];
+    unsigned long long nxt[8];
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+      const int sid = w[x];
+      nxt[x] = sid >= 0 ? *(const unsigned long long*)&p.spec[(fbase + sid) * kFB + f] : 0ull;
+    }
+    unsigned long long A[16], B[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) A[c] = B[c] = 0ull;
+    for (int row = 0; row < 36; ++row) {
+      unsigned long long sr[8], si[8];  // {sr, sr}, {si, si}
+#pragma unroll
+      for (int x = 0; x < 8; ++x) {
+        sr[x] = pack2(lo_of(nxt[x]), lo_of(nxt[x]));
+        si[x] = pack2(hi_of(nxt[x]), hi_of(nxt[x]));
+      }
+      if (row + 1 < 36) {
+#pragma unroll
+        for (int x = 0; x < 8; ++x) {
+          const int sid = w[(row + 1) * 8 + x];
+          nxt[x] =
+              sid >= 0 ? *(const unsigned long long*)&p.spec[(fbase + sid) * kFB + f] : 0ull;
+        }
+      }
+      const int wy = row % 6, wz = row / 6;
+#pragma unroll
+      for (int cyz = 0; cyz < 4; ++cyz) {
+        const int cy = cyz >> 1, cz = cyz & 1;
+        const unsigned long long* trow =
+            tsm + ((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * kFB + f;
+        unsigned long long t[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) t[k] = trow[k * kFB];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int wx = 0; wx < 6; ++wx)
+#pragma unroll
+            for (int cx = 0; cx < 2; ++cx) {
+              const int c = h * 8 + cx * 4 + cy * 2 + cz;
+              const unsigned long long tk = t[wx - cx + 1];
+              asm("fma.rn.f32x2 %0, %2, %3, %0;\n"
+                  "fma.rn.f32x2 %1, %2, %4, %1;\n"
+                  : "+l"(A[c]), "+l"(B[c])
+                  : "l"(tk), "l"(sr[wx + 2 * h]), "l"(si[wx + 2 * h]));
+            }
+      }
+      if (wy == 5) {  // end of a z-plane of the window
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          sums[(2 * c) * 32] += (double)lo_of(A[c]) - (double)hi_of(B[c]);
+          sums[(2 * c + 1) * 32] += (double)hi_of(A[c]) + (double)lo_of(B[c]);
+          A[c] = B[c] = 0ull;
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const int m = mem[slot][c];
+      if (m >= 0)
+        p.effv[(fbase + m) * kFB + f] =
+            make_float2((float)sums[(2 * c) * 32], (float)sums[(2 * c + 1) * 32]);
     }
     __syncwarp();
   }

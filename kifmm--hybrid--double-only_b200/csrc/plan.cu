@@ -103,6 +103,11 @@ struct kfmm_plan {
   int n_fft = 0, n_ifft = 0;
   int *win = nullptr, *members = nullptr;
   int n_groups = 0;
+  // mixed form: x-neighbour pairs of groups and the groups left single
+  int *pair_win = nullptr, *pair_members = nullptr, *single_win = nullptr,
+      *single_members = nullptr;
+  int n_pairs = 0, n_singles = 0;
+  int pair_per_block = 0;
   kfmm_stats stats{};
   int num_sms = 148;
   double* splitk = nullptr;   // split-K partial sums, shared by the level GEMMs
@@ -542,7 +547,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     std::vector<std::unordered_map<long long, int>> at(maxd + 1);
     for (int i = 0; i < nn; ++i)
       at[d->depth[i]][key_of(d->path[3 * i], d->path[3 * i + 1], d->path[3 * i + 2])] = i;
-    std::vector<int> win, mem;
+    std::vector<int> win, mem, gparent;
     for (int pn = 0; pn < nn; ++pn) {
       if (is_leaf(pn)) continue;
       int m[8], any = 0;
@@ -588,8 +593,58 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       }
       win.insert(win.end(), w, w + 216);
       mem.insert(mem.end(), m, m + 8);
+      gparent.push_back(pn);
     }
     p->n_groups = (int)mem.size() / 8;
+    if (p->prec == KFMM_MIXED && p->n_groups) {
+      // pair groups whose parents are x-neighbours (x even, x + 1): their
+      // windows share 4 of 6 x-positions and form one 8 x 6 x 6 window
+      // per parent depth: parent position -> group
+      std::vector<std::unordered_map<long long, int>> gat(maxd + 1);
+      for (int g = 0; g < p->n_groups; ++g) {
+        const int pn = gparent[g];
+        gat[d->depth[pn]][key_of(d->path[3 * pn], d->path[3 * pn + 1], d->path[3 * pn + 2])] = g;
+      }
+      std::vector<char> used(p->n_groups, 0);
+      std::vector<int> pwin, pmem, swin, smem;
+      for (int g = 0; g < p->n_groups; ++g) {
+        if (used[g]) continue;
+        const int pn = gparent[g];
+        int partner = -1;
+        if ((d->path[3 * pn] & 1) == 0) {
+          auto& level = gat[d->depth[pn]];
+          auto it = level.find(key_of(d->path[3 * pn] + 1, d->path[3 * pn + 1], d->path[3 * pn + 2]));
+          if (it != level.end() && !used[it->second]) partner = it->second;
+        }
+        used[g] = 1;
+        if (partner < 0) {
+          swin.insert(swin.end(), &win[(size_t)g * 216], &win[(size_t)g * 216] + 216);
+          smem.insert(smem.end(), &mem[(size_t)g * 8], &mem[(size_t)g * 8] + 8);
+          continue;
+        }
+        used[partner] = 1;
+        int w8[288];
+        for (int q = 0; q < 36; ++q)
+          for (int x = 0; x < 8; ++x) {
+            const int a = x < 6 ? win[(size_t)g * 216 + q * 6 + x] : -2;
+            const int b = x >= 2 ? win[(size_t)partner * 216 + q * 6 + x - 2] : -2;
+            if (a != -2 && b != -2 && a != b) {
+              set_error("kfmm_plan_create: neighbouring V-list windows disagree");
+              return KFMM_ERR_INVALID;
+            }
+            w8[q * 8 + x] = a != -2 ? a : b;
+          }
+        pwin.insert(pwin.end(), w8, w8 + 288);
+        pmem.insert(pmem.end(), &mem[(size_t)g * 8], &mem[(size_t)g * 8] + 8);
+        pmem.insert(pmem.end(), &mem[(size_t)partner * 8], &mem[(size_t)partner * 8] + 8);
+      }
+      p->n_pairs = (int)pmem.size() / 16;
+      p->n_singles = (int)smem.size() / 8;
+      KF_TRY(upload(p, &p->pair_win, pwin));
+      KF_TRY(upload(p, &p->pair_members, pmem));
+      KF_TRY(upload(p, &p->single_win, swin));
+      KF_TRY(upload(p, &p->single_members, smem));
+    }
     KF_TRY(upload(p, &p->win, win));
     KF_TRY(upload(p, &p->members, mem));
     p->stats.spectra_bytes = 16.0 * F * ((double)fn.size() + (double)ifn.size());
@@ -669,12 +724,19 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
                                (int)kGemmSmemBytes));
   KF_CUDA(cudaFuncSetAttribute(hadamard_fp32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kHad32TileBytes));
+  KF_CUDA(cudaFuncSetAttribute(hadamard_fp32_pair_kernel,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kHadPairSmemBytes));
   {
-    // about 8 waves of one CTA per SM over (group chunks x frequency blocks)
+    // about 8 waves of one CTA per SM over (chunks x frequency blocks)
     const int nfb = p->Fpad / kFB;
-    const int max_chunks = std::max(1, (p->n_groups + kHad32Warps - 1) / kHad32Warps);
-    const int chunks = std::max(1, std::min(max_chunks, (8 * p->num_sms + nfb - 1) / nfb));
-    p->had32_groups_per_block = (p->n_groups + chunks - 1) / chunks;
+    auto per_block = [&](int items, int warps) {
+      const int max_chunks = std::max(1, (items + warps - 1) / warps);
+      const int chunks = std::max(1, std::min(max_chunks, (8 * p->num_sms + nfb - 1) / nfb));
+      return std::max(1, (items + chunks - 1) / chunks);
+    };
+    p->had32_groups_per_block = per_block(p->n_singles, kHad32Warps);
+    p->pair_per_block = per_block(p->n_pairs, kHadPairWarps);
   }
 
   if (p->splitk_doubles) KF_TRY(dalloc(p, &p->splitk, p->splitk_doubles));
@@ -699,7 +761,9 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   for (const GemmBatch& b : p->up_gemms) reduces += b.nsplit > 1;
   for (const GemmBatch& b : p->down_gemms) reduces += b.nsplit > 1;
   p->stats.launches = reduces + (p->n_s2m > 0) + (int)p->up_gemms.size() + (p->n_fft > 0) +
-                      (p->n_groups > 0) + (p->n_ifft > 0) + (p->n_s2l > 0) +
+                      (p->prec == KFMM_MIXED ? (p->n_pairs > 0) + (p->n_singles > 0)
+                                             : (p->n_groups > 0)) +
+                      (p->n_ifft > 0) + (p->n_s2l > 0) +
                       (int)p->down_gemms.size() + (p->n_nf > 0) + 1;
   for (int i = 0; i < 7; ++i) KF_CUDA(cudaEventCreate(&p->ev[i]));
   return KFMM_OK;
@@ -881,13 +945,24 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
   }
   if (p->n_groups) {
     if (mixed) {
-      const int gpb = p->had32_groups_per_block;
-      Had32Params h{p->nn, p->n_groups, gpb, p->win, p->members,
-                    (const float2*)p->d_trans, (const float2*)p->spec, (float2*)p->effv,
-                    p->d_error};
-      dim3 grid((p->n_groups + gpb - 1) / gpb, p->Fpad / kFB);
-      hadamard_fp32_kernel<<<grid, kHad32Threads, kHad32TileBytes, S(stream)>>>(h);
-      KF_CHECK_LAUNCH("hadamard_fp32_kernel");
+      if (p->n_pairs) {
+        const int ppb = p->pair_per_block;
+        HadPairParams h{p->nn, p->n_pairs, ppb, p->pair_win, p->pair_members,
+                        (const float2*)p->d_trans, (const float2*)p->spec, (float2*)p->effv,
+                        p->d_error};
+        dim3 grid((p->n_pairs + ppb - 1) / ppb, p->Fpad / kFB);
+        hadamard_fp32_pair_kernel<<<grid, kHadPairThreads, kHadPairSmemBytes, S(stream)>>>(h);
+        KF_CHECK_LAUNCH("hadamard_fp32_pair_kernel");
+      }
+      if (p->n_singles) {
+        const int gpb = p->had32_groups_per_block;
+        Had32Params h{p->nn, p->n_singles, gpb, p->single_win, p->single_members,
+                      (const float2*)p->d_trans, (const float2*)p->spec, (float2*)p->effv,
+                      p->d_error};
+        dim3 grid((p->n_singles + gpb - 1) / gpb, p->Fpad / kFB);
+        hadamard_fp32_kernel<<<grid, kHad32Threads, kHad32TileBytes, S(stream)>>>(h);
+        KF_CHECK_LAUNCH("hadamard_fp32_kernel");
+      }
     } else {
       HadamardParams h{p->nn, p->n_groups, kHadGroupsPerBlock, p->win, p->members,
                        (const double2*)p->d_trans, p->Fpad, (const double2*)p->spec,
