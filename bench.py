@@ -39,6 +39,11 @@ FLOPS_PER_PAIR = 11.0   # reference convention, fmm/driver.cc:60
 # pool; the algorithmic bytes (sources, targets, potentials and downward
 # densities once each) are 348 MB.
 NEAR_FIELD_DRAM_BYTES = {"mixed": 354.8e6, "fp64": 357.1e6}
+# batched workload: independent solves, point counts log-uniform in
+# [4096, 262144], half uniform cube / half ellipsoid surface, NP in {3, 4},
+# leaf sizes from the autotuner, all solves in one CUDA graph
+BATCH_SOLVES = 256
+BATCH_LEAF_CANDIDATES = (32, 64, 128, 256)
 
 
 def parse():
@@ -49,6 +54,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_POINTS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-solves sub-measurement")
+    ap.add_argument("--batch", type=int, default=BATCH_SOLVES)
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="profile one form only (no JSON line)")
     return ap.parse_args()
@@ -224,6 +232,46 @@ def time_plan(K, plan, sh, stream, steps, warmup, barrier, world, dev):
     return ms, phases, statistics.median(nf_ms)
 
 
+def time_batched(K, count, stream, steps, warmup, dev):
+    """The batched workload in both forms: device time of one graph launch
+    (all solves), solves/s and Mpts/s, and per-solve error of the mixed form
+    against the plain one on a subset."""
+    import torch
+    from kifmm_b200 import autotune, batched
+    autotune.CANDIDATES = BATCH_LEAF_CANDIDATES
+    sp = batched.specs(count)
+    out = {"solves": count, "total_points": sum(s["n"] for s in sp),
+           "workload": "independent solves, N log-uniform in [4096, 262144], half uniform cube / "
+                       "half ellipsoid surface, NP in {3,4}, leaf size from the autotuner, one "
+                       "CUDA graph launch", "leaf_candidates": list(BATCH_LEAF_CANDIDATES)}
+    sh = stream.cuda_stream
+    pots = {}
+    for name, prec in (("mixed", K.MIXED), ("fp64", K.PLAIN_FP64)):
+        table = autotune.LeafSizeTable()
+        B = batched.BatchedSolves(K, sp, prec, table=table, nstreams=8)
+        for _ in range(warmup):
+            B.launch(sh)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            B.launch(sh)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / steps
+        pots[name] = B.potentials()
+        out[name] = {"ms_per_batch": ms, "solves_per_s": count / (ms * 1e-3),
+                     "Mpts_per_s": B.total_points / (ms * 1e-3) / 1e6,
+                     "leaf_sizes": {k: v["ppb"] for k, v in table.picks.items()}}
+        B.close()
+    rel = [float(np.linalg.norm(m - p) / np.linalg.norm(p)) for m, p in zip(pots["mixed"],
+                                                                            pots["fp64"])]
+    out["mixed_over_fp64"] = out["fp64"]["ms_per_batch"] / out["mixed"]["ms_per_batch"]
+    out["rel_l2_mixed_vs_fp64_max"] = max(rel)
+    out["rel_l2_mixed_vs_fp64_median"] = float(np.median(rel))
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -334,6 +382,11 @@ def main():
                 "peak_source": "kfmm_measure_peak micro-benchmark, this run",
                 "pairs_per_s": rate, "launch_ms": nf_ms}
 
+    batched_res = None
+    if not args.no_batched and args.batch > 0:
+        batched_res = time_batched(K, args.batch, stream, max(1, min(args.steps, 5)),
+                                   max(1, args.warmup), dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -368,6 +421,7 @@ def main():
         "tree": {"nodes": st["num_nodes"], "u_pairs": pairs, "v_pairs": st["v_pairs"]},
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
         "measured_pipes": pipes,
+        "batched": batched_res,
     }
     if rank == 0:
         print(json.dumps(line))

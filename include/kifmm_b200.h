@@ -204,6 +204,22 @@ kfmm_status kfmm_s2m_noalloc(int np, int nleaves, const double* src4, const int*
                              const int* leaf_num, const double* leaf_ctr, const double* uc2ue,
                              double* uden, void* stream);
 
+/* Batched solves (no counterpart in the reference, which runs one solve per
+ * process).  kfmm_batch_create captures kfmm_run of every plan into one CUDA
+ * graph whose branches are spread over `nstreams` concurrent streams (1 to
+ * 32); kfmm_batch_launch replays all solves with one graph launch on
+ * `stream`.  The plans keep their own device buffers: set their points
+ * (kfmm_set_sources/targets, or *_device) before a launch and read results
+ * with kfmm_copy_trg_val / kfmm_get_potentials_device after it.  Phase timing
+ * is switched off on the plans while they are captured.  A plan may belong to
+ * one batch at a time and must outlive it; calls on a batch are not
+ * re-entrant. */
+typedef struct kfmm_batch kfmm_batch;
+kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
+                              kfmm_batch** out);
+kfmm_status kfmm_batch_launch(kfmm_batch* batch, void* stream);
+kfmm_status kfmm_batch_destroy(kfmm_batch* batch);
+
 /* Throughput of the current device's execution pipes, measured by
  * micro-benchmarks (no reference counterpart; roofline denominators):
  * what 0: FP64 FMA TFLOP/s, 1: FP32 FMA TFLOP/s, 2: FP32 rsqrt 1e12/s (MUFU),

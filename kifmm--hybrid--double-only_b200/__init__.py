@@ -90,6 +90,9 @@ def lib():
         "kfmm_phase_times": [vp, ctypes.POINTER(ctypes.c_float)],
         "kfmm_measure_peak": [i, _f64p],
         "kfmm_s2m_noalloc": [i, i, vp, vp, vp, vp, vp, vp, vp],
+        "kfmm_batch_create": [ctypes.POINTER(vp), i, i, ctypes.POINTER(vp)],
+        "kfmm_batch_launch": [vp, vp],
+        "kfmm_batch_destroy": [vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -263,6 +266,34 @@ class Plan:
     def close(self):
         if self.handle:
             lib().kfmm_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many plans replayed by one CUDA graph launch (kfmm_batch_create).  The
+    plans must have their points set; they stay owned by the caller and must
+    outlive the batch."""
+
+    def __init__(self, plans, nstreams=8):
+        self.plans = list(plans)
+        arr = (ctypes.c_void_p * len(self.plans))(*[p.handle for p in self.plans])
+        h = ctypes.c_void_p()
+        check(lib().kfmm_batch_create(arr, len(self.plans), nstreams, ctypes.byref(h)),
+              "batch_create")
+        self.handle = h
+
+    def launch(self, stream=None):
+        check(lib().kfmm_batch_launch(self.handle, stream), "batch_launch")
+
+    def close(self):
+        if self.handle:
+            lib().kfmm_batch_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

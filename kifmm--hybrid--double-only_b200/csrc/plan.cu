@@ -1125,6 +1125,98 @@ kfmm_status kfmm_plan_stats(const kfmm_plan* p, kfmm_stats* s) {
   return KFMM_OK;
 }
 
+struct kfmm_batch {
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+static void batch_release(kfmm_batch* b) {
+  if (!b) return;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+  for (cudaStream_t s : b->streams) cudaStreamDestroy(s);
+  delete b;
+}
+
+kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
+                              kfmm_batch** out) {
+  if (!plans || !out || nplans < 1 || nstreams < 1 || nstreams > 32) {
+    set_error("kfmm_batch_create: need plans, nplans >= 1 and 1 <= nstreams <= 32");
+    return KFMM_ERR_INVALID;
+  }
+  *out = nullptr;
+  for (int i = 0; i < nplans; ++i)
+    if (!plans[i] || !plans[i]->have_src || !plans[i]->have_trg) {
+      set_error("kfmm_batch_create: plan " + std::to_string(i) + " is null or has no points");
+      return KFMM_ERR_STATE;
+    }
+  nstreams = std::min(nstreams, nplans);
+  kfmm_batch* b = new kfmm_batch();
+  auto fail = [&](cudaError_t e, const char* what) {
+    set_error(std::string("kfmm_batch_create: ") + what + ": " + cudaGetErrorString(e));
+    batch_release(b);
+    return KFMM_ERR_CUDA;
+  };
+  cudaError_t e;
+  b->streams.resize(nstreams + 1);
+  for (auto& st : b->streams) {
+    st = nullptr;
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess)
+      return fail(e, "cudaStreamCreate");
+  }
+  b->events.resize(nstreams + 1);
+  for (auto& ev : b->events) {
+    ev = nullptr;
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+      return fail(e, "cudaEventCreate");
+  }
+  cudaStream_t origin = b->streams[nstreams];
+  if ((e = cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return fail(e, "cudaStreamBeginCapture");
+  // fork: every branch stream waits on the origin, then runs its plans
+  cudaEventRecord(b->events[nstreams], origin);
+  for (int k = 0; k < nstreams; ++k) cudaStreamWaitEvent(b->streams[k], b->events[nstreams], 0);
+  kfmm_status st = KFMM_OK;
+  for (int i = 0; i < nplans && st == KFMM_OK; ++i) {
+    const bool timing = plans[i]->timing;
+    plans[i]->timing = false;
+    st = kfmm_run(plans[i], b->streams[i % nstreams]);
+    plans[i]->timing = timing;
+  }
+  // join
+  for (int k = 0; k < nstreams; ++k) {
+    cudaEventRecord(b->events[k], b->streams[k]);
+    cudaStreamWaitEvent(origin, b->events[k], 0);
+  }
+  e = cudaStreamEndCapture(origin, &b->graph);
+  if (st != KFMM_OK) {
+    batch_release(b);
+    return st;
+  }
+  if (e != cudaSuccess) return fail(e, "cudaStreamEndCapture");
+  if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess)
+    return fail(e, "cudaGraphInstantiate");
+  *out = b;
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_batch_launch(kfmm_batch* b, void* stream) {
+  if (!b || !b->exec) {
+    set_error("kfmm_batch_launch: null batch");
+    return KFMM_ERR_INVALID;
+  }
+  KF_CUDA(cudaGraphLaunch(b->exec, S(stream)));
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_batch_destroy(kfmm_batch* b) {
+  batch_release(b);
+  return KFMM_OK;
+}
+
 kfmm_status kfmm_enable_timing(kfmm_plan* p, int enable) {
   if (!p) return KFMM_ERR_INVALID;
   p->timing = enable != 0;

@@ -35,6 +35,7 @@ CASES = [
     ("ellipsoidSurface", 30000, 48, 4, 0),
     ("uniform", 12000, 40, 5, 1),
     ("ellipseUniformAngles", 6000, 16, 8, 0),
+    ("uniform", 65536, 128, 4, 1),  # the CPU-runnable benchmark configuration (fmmd--omp)
 ]
 
 
