@@ -17,9 +17,13 @@
 // method with high relative accuracy, in place of LAPACK DGESVD.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
 
 #include "host.h"
 
@@ -251,6 +255,95 @@ static void compute_operators(int np, Operators& op) {
       }
 }
 
+// On-disk operator cache.  With KFMM_OPERATOR_CACHE=<directory> set, the
+// operators of an NP are read from <directory>/kifmm_operators_np<NP>.bin when
+// that file is valid, else computed and written there (atomically: a
+// temporary file renamed into place).  File: magic, format version, NP,
+// pseudo-inverse cutoff exponent (np + 1), P, Q, F, the five arrays in
+// Operators order, then a 64-bit FNV-1a checksum of everything before it.  A
+// file with any other header, size or checksum is ignored and replaced.
+namespace {
+
+constexpr uint64_t kOpsMagic = 0x31534f504d4d464bull;  // "KFMMPOS1"
+constexpr int kOpsVersion = 1;
+
+uint64_t fnv1a(const void* data, size_t n, uint64_t h = 1469598103934665603ull) {
+  const unsigned char* p = (const unsigned char*)data;
+  for (size_t i = 0; i < n; ++i) h = (h ^ p[i]) * 1099511628211ull;
+  return h;
+}
+
+std::vector<std::vector<double>*> op_arrays(Operators& op) {
+  return {&op.uc2ue, &op.ue2uc, &op.dc2de, &op.de2dc, &op.ue2dc};
+}
+
+std::string cache_path(int np) {
+  const char* dir = std::getenv("KFMM_OPERATOR_CACHE");
+  if (!dir || !*dir) return std::string();
+  return std::string(dir) + "/kifmm_operators_np" + std::to_string(np) + ".bin";
+}
+
+bool load_operators(const std::string& path, int np, Operators& op) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return false;
+  std::vector<unsigned char> buf;
+  unsigned char tmp[1 << 16];
+  size_t got;
+  while ((got = std::fread(tmp, 1, sizeof tmp, f)) > 0) buf.insert(buf.end(), tmp, tmp + got);
+  std::fclose(f);
+  int64_t head[8];
+  if (buf.size() < sizeof head + 8) return false;
+  std::memcpy(head, buf.data(), sizeof head);
+  Operators want;
+  want.np = np;
+  want.P = np * np * np - (np - 2) * (np - 2) * (np - 2);
+  want.Q = (np + 2) * (np + 2) * (np + 2) - np * np * np;
+  want.F = (np + 1) * 4 * np * np;
+  const size_t sizes[5] = {(size_t)want.P * want.Q, (size_t)8 * want.Q * want.P,
+                           (size_t)want.P * want.P, (size_t)8 * want.P * want.P,
+                           (size_t)343 * 2 * want.F};
+  size_t total = 0;
+  for (size_t z : sizes) total += z;
+  if ((uint64_t)head[0] != kOpsMagic || head[1] != kOpsVersion || head[2] != np ||
+      head[3] != np + 1 || head[4] != want.P || head[5] != want.Q || head[6] != want.F ||
+      head[7] != (int64_t)total || buf.size() != sizeof head + 8 * total + 8)
+    return false;
+  uint64_t sum;
+  std::memcpy(&sum, buf.data() + buf.size() - 8, 8);
+  if (fnv1a(buf.data(), buf.size() - 8) != sum) return false;
+  const unsigned char* p = buf.data() + sizeof head;
+  auto arrays = op_arrays(want);
+  for (int k = 0; k < 5; ++k) {
+    arrays[k]->resize(sizes[k]);
+    std::memcpy(arrays[k]->data(), p, 8 * sizes[k]);
+    p += 8 * sizes[k];
+  }
+  op = std::move(want);
+  return true;
+}
+
+void store_operators(const std::string& path, Operators& op) {
+  std::vector<unsigned char> buf;
+  size_t total = 0;
+  for (auto* a : op_arrays(op)) total += a->size();
+  const int64_t head[8] = {(int64_t)kOpsMagic, kOpsVersion, op.np, op.np + 1,
+                           op.P,               op.Q,        op.F,  (int64_t)total};
+  buf.insert(buf.end(), (const unsigned char*)head, (const unsigned char*)head + sizeof head);
+  for (auto* a : op_arrays(op))
+    buf.insert(buf.end(), (const unsigned char*)a->data(),
+               (const unsigned char*)(a->data() + a->size()));
+  const uint64_t sum = fnv1a(buf.data(), buf.size());
+  buf.insert(buf.end(), (const unsigned char*)&sum, (const unsigned char*)&sum + 8);
+  const std::string tmp = path + ".tmp" + std::to_string((long long)std::rand());
+  FILE* f = std::fopen(tmp.c_str(), "wb");
+  if (!f) return;  // the cache is an optimisation: failures leave it alone
+  const bool ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  if (std::fclose(f) == 0 && ok) std::rename(tmp.c_str(), path.c_str());
+  else std::remove(tmp.c_str());
+}
+
+}  // namespace
+
 const Operators& operators_for(int np) {
   static std::mutex mu;
   static std::map<int, Operators> cache;
@@ -258,7 +351,10 @@ const Operators& operators_for(int np) {
   auto it = cache.find(np);
   if (it != cache.end()) return it->second;
   Operators& op = cache[np];
+  const std::string path = cache_path(np);
+  if (!path.empty() && load_operators(path, np, op)) return op;
   compute_operators(np, op);
+  if (!path.empty()) store_operators(path, op);
   return op;
 }
 
