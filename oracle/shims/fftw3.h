@@ -38,6 +38,22 @@ void fftw_execute_dft_r2c(const fftw_plan p, double* in, fftw_complex* out);
 void fftw_execute_dft_c2r(const fftw_plan p, fftw_complex* in, double* out);
 void fftw_destroy_plan(fftw_plan p);
 
+/* single precision (the reference's USE_FLOAT build, fmm/reals_aligned.h:123-134) */
+typedef float fftwf_complex[2];
+typedef struct kfmm_shim_fftwf_plan_s* fftwf_plan;
+fftwf_plan fftwf_plan_many_dft_r2c(int rank, const int* n, int howmany,
+                                   float* in, const int* inembed, int istride, int idist,
+                                   fftwf_complex* out, const int* onembed, int ostride,
+                                   int odist, unsigned flags);
+fftwf_plan fftwf_plan_many_dft_c2r(int rank, const int* n, int howmany,
+                                   fftwf_complex* in, const int* inembed, int istride,
+                                   int idist, float* out, const int* onembed, int ostride,
+                                   int odist, unsigned flags);
+void fftwf_execute(const fftwf_plan p);
+void fftwf_execute_dft_r2c(const fftwf_plan p, float* in, fftwf_complex* out);
+void fftwf_execute_dft_c2r(const fftwf_plan p, fftwf_complex* in, float* out);
+void fftwf_destroy_plan(fftwf_plan p);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,6 +1,7 @@
 /*
  * Test infrastructure (oracle build only).  Separable discrete Fourier
- * transforms that stand in for FFTW 3.2.2's r2c / c2r plans in the reference
+ * transforms that stand in for FFTW 3.2.2's r2c / c2r plans (double, and
+ * single precision for the reference's USE_FLOAT build) in the reference
  * CPU build.  Each 1-D pass is a direct DFT with twiddles exp(+-2*pi*i*m/n)
  * tabulated once per plan from libm cos/sin; the 3-D transform is the usual
  * row-column composition (last dimension first for r2c, last dimension last
@@ -16,25 +17,41 @@
 
 #include "fftw3.h"
 
+/* One source, two instances: FFTW's double API (fftw_*) by default, its
+   single-precision API (fftwf_*, arithmetic in float) with -DSHIM_FLOAT. */
+#ifdef SHIM_FLOAT
+#define SR float
+#define SC fftwf_complex
+#define SP fftwf_plan
+#define PLAN_S kfmm_shim_fftwf_plan_s
+#define SNAME(x) fftwf_##x
+#else
+#define SR double
+#define SC fftw_complex
+#define SP fftw_plan
+#define PLAN_S kfmm_shim_fftw_plan_s
+#define SNAME(x) fftw_##x
+#endif
+
 #define SHIM_MAXN 32
 
-struct kfmm_shim_fftw_plan_s {
+struct PLAN_S {
   int dir; /* -1: r2c forward, +1: c2r backward */
   int n0, n1, n2, h2; /* h2 = n2/2 + 1 */
-  double* rbuf;       /* real array bound at plan time */
-  fftw_complex* cbuf; /* complex array bound at plan time */
-  double cs[3][SHIM_MAXN]; /* cos(2 pi m / n_d) */
-  double sn[3][SHIM_MAXN]; /* sin(2 pi m / n_d) */
+  SR* rbuf;       /* real array bound at plan time */
+  SC* cbuf; /* complex array bound at plan time */
+  SR cs[3][SHIM_MAXN]; /* cos(2 pi m / n_d) */
+  SR sn[3][SHIM_MAXN]; /* sin(2 pi m / n_d) */
 };
 
-static struct kfmm_shim_fftw_plan_s* make_plan(int rank, const int* n, int howmany,
+static struct PLAN_S* make_plan(int rank, const int* n, int howmany,
                                                int istride, int idist, int ostride,
                                                int odist, int dir) {
   assert(rank == 3 && howmany == 1 && istride == 1 && ostride == 1);
   (void)idist;
   (void)odist;
-  struct kfmm_shim_fftw_plan_s* p =
-      (struct kfmm_shim_fftw_plan_s*)calloc(1, sizeof(*p));
+  struct PLAN_S* p =
+      (struct PLAN_S*)calloc(1, sizeof(*p));
   assert(p);
   p->dir = dir;
   p->n0 = n[0];
@@ -52,28 +69,28 @@ static struct kfmm_shim_fftw_plan_s* make_plan(int rank, const int* n, int howma
   return p;
 }
 
-fftw_plan fftw_plan_many_dft_r2c(int rank, const int* n, int howmany, double* in,
+SP SNAME(plan_many_dft_r2c)(int rank, const int* n, int howmany, SR* in,
                                  const int* inembed, int istride, int idist,
-                                 fftw_complex* out, const int* onembed, int ostride,
+                                 SC* out, const int* onembed, int ostride,
                                  int odist, unsigned flags) {
   (void)inembed;
   (void)onembed;
   (void)flags;
-  struct kfmm_shim_fftw_plan_s* p =
+  struct PLAN_S* p =
       make_plan(rank, n, howmany, istride, idist, ostride, odist, -1);
   p->rbuf = in;
   p->cbuf = out;
   return p;
 }
 
-fftw_plan fftw_plan_many_dft_c2r(int rank, const int* n, int howmany, fftw_complex* in,
-                                 const int* inembed, int istride, int idist, double* out,
+SP SNAME(plan_many_dft_c2r)(int rank, const int* n, int howmany, SC* in,
+                                 const int* inembed, int istride, int idist, SR* out,
                                  const int* onembed, int ostride, int odist,
                                  unsigned flags) {
   (void)inembed;
   (void)onembed;
   (void)flags;
-  struct kfmm_shim_fftw_plan_s* p =
+  struct PLAN_S* p =
       make_plan(rank, n, howmany, istride, idist, ostride, odist, +1);
   p->cbuf = in;
   p->rbuf = out;
@@ -81,15 +98,15 @@ fftw_plan fftw_plan_many_dft_c2r(int rank, const int* n, int howmany, fftw_compl
 }
 
 /* complex 1-D DFT of length n along a strided line, in place via scratch */
-static void cdft_line(double* re, double* im, int stride, int n, const double* cs,
-                      const double* sn, int sign) {
-  double tr[SHIM_MAXN], ti[SHIM_MAXN];
+static void cdft_line(SR* re, SR* im, int stride, int n, const SR* cs,
+                      const SR* sn, int sign) {
+  SR tr[SHIM_MAXN], ti[SHIM_MAXN];
   for (int k = 0; k < n; ++k) {
-    double ar = 0.0, ai = 0.0;
+    SR ar = 0.0, ai = 0.0;
     for (int x = 0; x < n; ++x) {
       int m = (k * x) % n;
-      double c = cs[m], s = sign * sn[m];
-      double xr = re[x * stride], xi = im[x * stride];
+      SR c = cs[m], s = sign * sn[m];
+      SR xr = re[x * stride], xi = im[x * stride];
       ar += xr * c - xi * s;
       ai += xr * s + xi * c;
     }
@@ -102,18 +119,18 @@ static void cdft_line(double* re, double* im, int stride, int n, const double* c
   }
 }
 
-void fftw_execute_dft_r2c(const fftw_plan p, double* in, fftw_complex* out) {
+void SNAME(execute_dft_r2c)(const SP p, SR* in, SC* out) {
   const int n0 = p->n0, n1 = p->n1, n2 = p->n2, h2 = p->h2;
   const int nc = n0 * n1 * h2;
-  double* re = (double*)malloc(sizeof(double) * (size_t)nc);
-  double* im = (double*)malloc(sizeof(double) * (size_t)nc);
+  SR* re = (SR*)malloc(sizeof(SR) * (size_t)nc);
+  SR* im = (SR*)malloc(sizeof(SR) * (size_t)nc);
   assert(re && im);
   /* last dimension: real -> half complex, sign -1 */
   for (int a = 0; a < n0; ++a)
     for (int b = 0; b < n1; ++b) {
-      const double* row = in + ((size_t)a * n1 + b) * n2;
+      const SR* row = in + ((size_t)a * n1 + b) * n2;
       for (int k = 0; k < h2; ++k) {
-        double ar = 0.0, ai = 0.0;
+        SR ar = 0.0, ai = 0.0;
         for (int x = 0; x < n2; ++x) {
           int m = (k * x) % n2;
           ar += row[x] * p->cs[2][m];
@@ -141,11 +158,11 @@ void fftw_execute_dft_r2c(const fftw_plan p, double* in, fftw_complex* out) {
   free(im);
 }
 
-void fftw_execute_dft_c2r(const fftw_plan p, fftw_complex* in, double* out) {
+void SNAME(execute_dft_c2r)(const SP p, SC* in, SR* out) {
   const int n0 = p->n0, n1 = p->n1, n2 = p->n2, h2 = p->h2;
   const int nc = n0 * n1 * h2;
-  double* re = (double*)malloc(sizeof(double) * (size_t)nc);
-  double* im = (double*)malloc(sizeof(double) * (size_t)nc);
+  SR* re = (SR*)malloc(sizeof(SR) * (size_t)nc);
+  SR* im = (SR*)malloc(sizeof(SR) * (size_t)nc);
   assert(re && im);
   for (int i = 0; i < nc; ++i) {
     re[i] = in[i][0];
@@ -163,11 +180,11 @@ void fftw_execute_dft_c2r(const fftw_plan p, fftw_complex* in, double* out) {
   /* last dimension: Hermitian half complex -> real */
   for (int a = 0; a < n0; ++a)
     for (int b = 0; b < n1; ++b) {
-      const double* yr = re + ((size_t)a * n1 + b) * h2;
-      const double* yi = im + ((size_t)a * n1 + b) * h2;
-      double* row = out + ((size_t)a * n1 + b) * n2;
+      const SR* yr = re + ((size_t)a * n1 + b) * h2;
+      const SR* yi = im + ((size_t)a * n1 + b) * h2;
+      SR* row = out + ((size_t)a * n1 + b) * n2;
       for (int x = 0; x < n2; ++x) {
-        double acc = yr[0];
+        SR acc = yr[0];
         int kmax = (n2 % 2 == 0) ? n2 / 2 - 1 : n2 / 2;
         for (int k = 1; k <= kmax; ++k) {
           int m = (k * x) % n2;
@@ -181,11 +198,11 @@ void fftw_execute_dft_c2r(const fftw_plan p, fftw_complex* in, double* out) {
   free(im);
 }
 
-void fftw_execute(const fftw_plan p) {
+void SNAME(execute)(const SP p) {
   if (p->dir < 0)
-    fftw_execute_dft_r2c(p, p->rbuf, p->cbuf);
+    SNAME(execute_dft_r2c)(p, p->rbuf, p->cbuf);
   else
-    fftw_execute_dft_c2r(p, p->cbuf, p->rbuf);
+    SNAME(execute_dft_c2r)(p, p->cbuf, p->rbuf);
 }
 
-void fftw_destroy_plan(fftw_plan p) { free(p); }
+void SNAME(destroy_plan)(SP p) { free(p); }

@@ -29,6 +29,19 @@ void DGEMV(const char* trans, const int* m, const int* n, const double* alpha,
 void DAXPY(const int* n, const double* alpha, const double* x, const int* incx,
            double* y, const int* incy);
 
+/* single precision, for the reference's USE_FLOAT build (fmm/reals_aligned.h:136-139) */
+void SGESVD(const char* jobu, const char* jobvt, const int* m, const int* n, float* a,
+            const int* lda, float* s, float* u, const int* ldu, float* vt, const int* ldvt,
+            float* work, const int* lwork, int* info);
+void SGEMM(const char* transa, const char* transb, const int* m, const int* n, const int* k,
+           const float* alpha, const float* a, const int* lda, const float* b, const int* ldb,
+           const float* beta, float* c, const int* ldc);
+void SGEMV(const char* trans, const int* m, const int* n, const float* alpha, const float* a,
+           const int* lda, const float* x, const int* incx, const float* beta, float* y,
+           const int* incy);
+void SAXPY(const int* n, const float* alpha, const float* x, const int* incx, float* y,
+           const int* incy);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,3 +46,41 @@ void DAXPY(const int* n, const double* alpha, const double* x, const int* incx,
            double* y, const int* incy) {
   for (int i = 0; i < *n; ++i) y[(size_t)i * *incy] += *alpha * x[(size_t)i * *incx];
 }
+
+/* single precision (USE_FLOAT build) */
+extern void scipy_sgesvd_(const char*, const char*, const int*, const int*, float*, const int*,
+                          float*, float*, const int*, float*, const int*, float*, const int*,
+                          int*, size_t, size_t);
+extern void scipy_sgemm_(const char*, const char*, const int*, const int*, const int*,
+                         const float*, const float*, const int*, const float*, const int*,
+                         const float*, float*, const int*, size_t, size_t);
+
+void SGESVD(const char* jobu, const char* jobvt, const int* m, const int* n, float* a,
+            const int* lda, float* s, float* u, const int* ldu, float* vt, const int* ldvt,
+            float* work, const int* lwork, int* info) {
+  scipy_sgesvd_(jobu, jobvt, m, n, a, lda, s, u, ldu, vt, ldvt, work, lwork, info, 1, 1);
+}
+
+void SGEMM(const char* transa, const char* transb, const int* m, const int* n, const int* k,
+           const float* alpha, const float* a, const int* lda, const float* b, const int* ldb,
+           const float* beta, float* c, const int* ldc) {
+  scipy_sgemm_(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, 1, 1);
+}
+
+void SGEMV(const char* trans, const int* m, const int* n, const float* alpha, const float* a,
+           const int* lda, const float* x, const int* incx, const float* beta, float* y,
+           const int* incy) {
+  assert((*trans == 'N' || *trans == 'n') && *incx == 1 && *incy == 1);
+  const int M = *m, N = *n, LD = *lda;
+  for (int i = 0; i < M; ++i) y[i] *= *beta;
+  for (int j = 0; j < N; ++j) {
+    const float t = *alpha * x[j];
+    const float* col = a + (size_t)j * LD;
+    for (int i = 0; i < M; ++i) y[i] += t * col[i];
+  }
+}
+
+void SAXPY(const int* n, const float* alpha, const float* x, const int* incx, float* y,
+           const int* incy) {
+  for (int i = 0; i < *n; ++i) y[(size_t)i * *incy] += *alpha * x[(size_t)i * *incx];
+}
