@@ -297,7 +297,16 @@ def main():
 
     # ---- setup (untimed): points, tree + lists, plans (operators, device arrays)
     pts = K.generate_points(n, DIST, 0, replica_seed(rank), 1000)
-    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], PPB)
+    targs = [pts[k] for k in ("sx", "sy", "sz", "tx", "ty", "tz")]
+    t0 = time.time()
+    tree = K.Tree(*targs, PPB)
+    tree_host_s = time.time() - t0
+    tree_device_s = None
+    if not args.only:
+        K.Tree(*targs, PPB, device=True).close()  # CUDA start-up and first-call costs
+        t0 = time.time()
+        K.Tree(*targs, PPB, device=True).close()
+        tree_device_s = time.time() - t0
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
     if args.only:
@@ -418,7 +427,8 @@ def main():
                 "h2d_bytes_per_step": 7 * 8 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": int(st["launches"]) * args.steps,
         "clocks": clk,
-        "tree": {"nodes": st["num_nodes"], "u_pairs": pairs, "v_pairs": st["v_pairs"]},
+        "tree": {"nodes": st["num_nodes"], "u_pairs": pairs, "v_pairs": st["v_pairs"],
+                 "build_s_host": tree_host_s, "build_s_device": tree_device_s},
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
         "measured_pipes": pipes,
         "batched": batched_res,

@@ -77,6 +77,16 @@ kfmm_status kfmm_tree_build(int num_src, const double* sx, const double* sy,
                             const double* sz, int num_trg, const double* tx,
                             const double* ty, const double* tz, int pts_max,
                             kfmm_tree** out);
+/* The same tree as kfmm_tree_build (identical description), with the point
+ * work done on the current CUDA device on `stream`: exact Morton keys of
+ * the reference's octant comparisons, radix sorts, a breadth-first split
+ * over the sorted keys; lists on the host (fmm/input.cc:204-460, replaced
+ * by this GPU path).  Trees of more than 21 levels give
+ * KFMM_ERR_UNSUPPORTED.  Host input arrays. */
+kfmm_status kfmm_tree_build_device(int num_src, const double* sx, const double* sy,
+                                   const double* sz, int num_trg, const double* tx,
+                                   const double* ty, const double* tz, int pts_max,
+                                   void* stream, kfmm_tree** out);
 kfmm_status kfmm_tree_describe(const kfmm_tree* tree, kfmm_tree_desc* desc);
 void kfmm_tree_destroy(kfmm_tree* tree);
 

@@ -64,6 +64,8 @@ def lib():
         "kfmm_tree_build": [i, _f64p, _f64p, _f64p, i, _f64p, _f64p, _f64p, i,
                             ctypes.POINTER(vp)],
         "kfmm_tree_describe": [vp, ctypes.POINTER(TreeDesc)],
+        "kfmm_tree_build_device": [i, _f64p, _f64p, _f64p, i, _f64p, _f64p, _f64p, i, vp,
+                                   ctypes.POINTER(vp)],
         "kfmm_sizes": [i, _i32p, _i32p, _i32p],
         "kfmm_operators": [i, _f64p, _f64p, _f64p, _f64p, _f64p],
         "kfmm_plan_create": [ctypes.POINTER(TreeDesc), i, i, ctypes.POINTER(vp)],
@@ -160,12 +162,19 @@ def operators(np_):
 class Tree:
     """Octree + interaction lists built by the library (fmm/input.cc)."""
 
-    def __init__(self, sx, sy, sz, tx, ty, tz, pts_max):
+    def __init__(self, sx, sy, sz, tx, ty, tz, pts_max, device=False, stream=None):
+        """device=True builds with the point work on the GPU
+        (kfmm_tree_build_device); the result is the same tree."""
         self._arrays = [np.ascontiguousarray(a, np.float64) for a in (sx, sy, sz, tx, ty, tz)]
         sx, sy, sz, tx, ty, tz = self._arrays
         h = ctypes.c_void_p()
-        check(lib().kfmm_tree_build(len(sx), _p(sx), _p(sy), _p(sz), len(tx), _p(tx), _p(ty),
-                                    _p(tz), pts_max, ctypes.byref(h)), "tree_build")
+        if device:
+            check(lib().kfmm_tree_build_device(len(sx), _p(sx), _p(sy), _p(sz), len(tx), _p(tx),
+                                               _p(ty), _p(tz), pts_max, stream, ctypes.byref(h)),
+                  "tree_build_device")
+        else:
+            check(lib().kfmm_tree_build(len(sx), _p(sx), _p(sy), _p(sz), len(tx), _p(tx), _p(ty),
+                                        _p(tz), pts_max, ctypes.byref(h)), "tree_build")
         self.handle = h
         self.desc = TreeDesc()
         check(lib().kfmm_tree_describe(h, ctypes.byref(self.desc)), "tree_describe")

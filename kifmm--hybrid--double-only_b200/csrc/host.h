@@ -29,6 +29,8 @@ struct Tree {
   std::vector<int> list_ptr[4], list_idx[4];  // U, V, W, X
   int num_nodes() const { return (int)parent.size(); }
 };
+// Fills T.list_ptr / list_idx from the tree structure and tags.
+void build_lists(Tree& T);
 
 // Surface sample grids and regular grid (fmm/trans.cc:14-88).
 struct Surfaces {

@@ -245,21 +245,31 @@ static void build_tree(Tree& T, int ns, const double* sx, const double* sy, cons
       T.trg_perm.insert(T.trg_perm.end(), tperm.begin() + tb[i], tperm.begin() + te[i]);
     }
   }
-  // Lists for every target-bearing node.
+  build_lists(T);
+}
+
+// U/V/W/X lists of every target-bearing node (nodes are independent: built in
+// parallel, concatenated in node order).
+void build_lists(Tree& T) {
+  const int nn = T.num_nodes();
   Builder B(T);
-  std::vector<int> L[4];
+  std::vector<std::vector<int>> per(4 * (size_t)nn);
+#pragma omp parallel
+  {
+    std::vector<int> L[4];
+#pragma omp for schedule(dynamic, 64)
+    for (int i = 0; i < nn; ++i) {
+      if (!(T.tag[i] & kTrgTag)) continue;
+      B.lists_of(i, L);
+      for (int k = 0; k < 4; ++k) per[4 * (size_t)i + k] = L[k];
+    }
+  }
   for (int k = 0; k < 4; ++k) {
     T.list_ptr[k].assign(1, 0);
     T.list_idx[k].clear();
-  }
-  for (int i = 0; i < nn; ++i) {
-    if (T.tag[i] & kTrgTag) {
-      B.lists_of(i, L);
-    } else {
-      for (int k = 0; k < 4; ++k) L[k].clear();
-    }
-    for (int k = 0; k < 4; ++k) {
-      T.list_idx[k].insert(T.list_idx[k].end(), L[k].begin(), L[k].end());
+    for (int i = 0; i < nn; ++i) {
+      const std::vector<int>& v = per[4 * (size_t)i + k];
+      T.list_idx[k].insert(T.list_idx[k].end(), v.begin(), v.end());
       T.list_ptr[k].push_back((int)T.list_idx[k].size());
     }
   }
