@@ -468,13 +468,17 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     int kind = ent >> 28, node = ent & 0x0fffffff;
     return kind == 0 ? d->src_num[node] : P;
   };
-  // largest first (target slots x sources) for the persistent P2P kernel
+  // For the persistent P2P kernel: largest first, by cost class (target slots
+  // x sources, in classes 25% wide); within a class the jobs keep their tree
+  // order, so warps working at the same time read neighbouring leaves' sources
+  // and the L2 cache serves the repeats.
   auto order_jobs = [&](std::vector<P2PJob>& jobs, const std::vector<int>& ent) {
     std::vector<std::pair<double, int>> key(jobs.size());
     for (size_t j = 0; j < jobs.size(); ++j) {
       double ns = 0;
       for (int k = jobs[j].ebeg; k < jobs[j].eend; ++k) ns += src_count(ent[k]);
-      key[j] = {-ns * ((jobs[j].tcnt + 31) / 32), (int)j};
+      const double cost = std::max(1.0, ns * ((jobs[j].tcnt + 31) / 32));
+      key[j] = {-std::floor(std::log(cost) / std::log(1.25)), (int)j};
     }
     std::stable_sort(key.begin(), key.end(),
                      [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
