@@ -230,6 +230,23 @@ kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
 kfmm_status kfmm_batch_launch(kfmm_batch* batch, void* stream);
 kfmm_status kfmm_batch_destroy(kfmm_batch* batch);
 
+/* Cost-model network (no counterpart in the reference, which takes the leaf
+ * size from its command line): a 3-layer perceptron in FP32,
+ *   Y = relu(relu(X W1 + b1) W2 + b2) W3 + b3,  X: B x F, hidden H, Y: B x O,
+ * trained on the GPU by hand-written forward, backward and Adam kernels on
+ * the loss mean((Y - T)^2).  params: packed [W1 | b1 | W2 | b2 | W3 | b3],
+ * weights row-major (input index major), kfmm_mlp_param_count floats; grads
+ * in the same layout.  Host arrays; the calls synchronise.  kfmm_mlp_train
+ * runs `steps` full-batch Adam steps (lr, beta 0.9 / 0.999), updates params
+ * in place and writes each step's loss to losses (may be NULL). */
+kfmm_status kfmm_mlp_param_count(int F, int H, int O, long long* count);
+kfmm_status kfmm_mlp_forward(int F, int H, int O, const float* params, int B, const float* X,
+                             float* Y);
+kfmm_status kfmm_mlp_gradients(int F, int H, int O, const float* params, int B,
+                               const float* X, const float* T, float* grads, float* loss);
+kfmm_status kfmm_mlp_train(int F, int H, int O, float* params, int B, const float* X,
+                           const float* T, int steps, float lr, float* losses);
+
 /* Throughput of the current device's execution pipes, measured by
  * micro-benchmarks (no reference counterpart; roofline denominators):
  * what 0: FP64 FMA TFLOP/s, 1: FP32 FMA TFLOP/s, 2: FP32 rsqrt 1e12/s (MUFU),

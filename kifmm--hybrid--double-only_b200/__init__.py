@@ -24,6 +24,7 @@ _lib = None
 
 _i32p = ctypes.POINTER(ctypes.c_int)
 _f64p = ctypes.POINTER(ctypes.c_double)
+_f32p = ctypes.POINTER(ctypes.c_float)
 
 
 class KfmmError(RuntimeError):
@@ -95,6 +96,10 @@ def lib():
         "kfmm_batch_create": [ctypes.POINTER(vp), i, i, ctypes.POINTER(vp)],
         "kfmm_batch_launch": [vp, vp],
         "kfmm_batch_destroy": [vp],
+        "kfmm_mlp_param_count": [i, i, i, ctypes.POINTER(ctypes.c_longlong)],
+        "kfmm_mlp_forward": [i, i, i, _f32p, i, _f32p, _f32p],
+        "kfmm_mlp_gradients": [i, i, i, _f32p, i, _f32p, _f32p, _f32p, _f32p],
+        "kfmm_mlp_train": [i, i, i, _f32p, i, _f32p, _f32p, i, ctypes.c_float, _f32p],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -310,3 +315,48 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class MLP:
+    """The cost-model network (kfmm_mlp_*): F inputs, H hidden, O outputs,
+    FP32 parameters held on the host, every computation on the GPU."""
+
+    def __init__(self, F, H, O, params=None, seed=0):
+        self.F, self.H, self.O = F, H, O
+        n = ctypes.c_longlong()
+        check(lib().kfmm_mlp_param_count(F, H, O, ctypes.byref(n)), "mlp_param_count")
+        self.n = n.value
+        if params is None:
+            rng = np.random.default_rng(seed)
+            parts = []
+            for fi, fo in ((F, H), (H, H), (H, O)):
+                parts += [rng.normal(0, np.sqrt(2.0 / fi), fi * fo), np.zeros(fo)]
+            params = np.concatenate(parts)
+        self.params = np.ascontiguousarray(params, np.float32)
+        assert self.params.size == self.n
+
+    def forward(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.empty((X.shape[0], self.O), np.float32)
+        check(lib().kfmm_mlp_forward(self.F, self.H, self.O, _p(self.params, _f32p), X.shape[0],
+                                     _p(X, _f32p), _p(Y, _f32p)), "mlp_forward")
+        return Y
+
+    def gradients(self, X, T):
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        g = np.empty(self.n, np.float32)
+        loss = ctypes.c_float()
+        check(lib().kfmm_mlp_gradients(self.F, self.H, self.O, _p(self.params, _f32p),
+                                       X.shape[0], _p(X, _f32p), _p(T, _f32p), _p(g, _f32p),
+                                       ctypes.byref(loss)), "mlp_gradients")
+        return g, loss.value
+
+    def train(self, X, T, steps, lr=1e-3):
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        losses = np.empty(steps, np.float32)
+        check(lib().kfmm_mlp_train(self.F, self.H, self.O, _p(self.params, _f32p), X.shape[0],
+                                   _p(X, _f32p), _p(T, _f32p), steps, lr, _p(losses, _f32p)),
+              "mlp_train")
+        return losses

@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, "libkifmm_b200.so")
 CLI = os.path.join(HERE, "fmmd--b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["plan.cu", "peaks.cu", "noalloc.cu", "tree.cc", "tree_gpu.cu", "operators.cc"]
+SOURCES = ["plan.cu", "peaks.cu", "noalloc.cu", "tree.cc", "tree_gpu.cu", "operators.cc", "mlp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
           "-Xcompiler", "-fPIC,-ffp-contract=off,-fopenmp"]

@@ -1,0 +1,282 @@
+"""Learned cost model for the leaf size (points per box).
+
+A small network (kfmm_mlp_*: 3 layers, 64 hidden units, FP32, trained and
+evaluated by this library's own CUDA kernels) maps tree statistics to the
+per-phase device times of one solve.  To pick the leaf size of a new cloud,
+the tree is built for every candidate (on the GPU, kfmm_tree_build_device:
+no plan, no solve), the network predicts each candidate's time, and the
+fastest prediction wins.  When the two best predictions are closer than
+`fallback_margin` (10%), those two candidates are measured and the faster
+one is taken: measurement stays the fallback, and the exhaustive measured
+sweep (autotune.best_leaf_size) the judge the model is scored against.
+
+Features of a (cloud, leaf size) tree: log point count, log leaf size, NP,
+node counts per level (16 levels), histograms of the U, V, W and X list
+lengths over target nodes (8 log2 bins each, as fractions), the log totals
+of U-list point pairs and V, W, X box pairs, and the logs of the near-field
+pairs padded to the kernel's 32-target granularity, of the box, leaf and
+V-list-box counts.  Targets: log(ms) of the
+phases up, vlist, xlist, down, ulist (kfmm_phase_times).
+
+Clouds (``make_cloud``): the uniform cube, the ellipsoid surface, and
+mixtures of 1 to 32 isotropic Gaussian clusters with sigma log-uniform in
+[0.005, 0.1] (points outside the root box redrawn).
+"""
+import json
+import math
+import os
+
+import numpy as np
+
+PHASES = ("up", "vlist", "xlist", "down", "ulist")
+LEAF_SIZES = (32, 64, 128, 256, 512, 1024)
+NLEVELS = 16
+NBINS = 8
+
+
+def cluster_points(n, k, sigma, rng):
+    centres = rng.uniform(-0.7, 0.7, (k, 3))
+    out = np.empty((n, 3))
+    filled = 0
+    while filled < n:
+        m = n - filled
+        c = centres[rng.integers(0, k, m)]
+        p = c + rng.normal(0.0, sigma, (m, 3))
+        ok = np.all((p >= -1.0) & (p < 1.0), axis=1)
+        p = p[ok]
+        out[filled:filled + len(p)] = p
+        filled += len(p)
+    return out
+
+
+def make_cloud(K, kind, n, seed):
+    """Points dict (sx..tz, den) for kind 'uniform', 'ellipsoidSurface' or
+    'clusters' (cluster count and width drawn from the seed)."""
+    if kind in ("uniform", "ellipsoidSurface"):
+        return K.generate_points(n, kind, 0, seed)
+    rng = np.random.default_rng(seed)
+    k = int(rng.integers(1, 33))
+    sigma = float(np.exp(rng.uniform(np.log(0.005), np.log(0.1))))
+    s = cluster_points(n, k, sigma, rng)
+    t = cluster_points(n, k, sigma, np.random.default_rng(seed + 7919))
+    return {"sx": s[:, 0].copy(), "sy": s[:, 1].copy(), "sz": s[:, 2].copy(),
+            "tx": t[:, 0].copy(), "ty": t[:, 1].copy(), "tz": t[:, 2].copy(),
+            "den": rng.uniform(0, 1, n), "clusters": k, "sigma": sigma}
+
+
+def _hist(lengths):
+    h = np.zeros(NBINS)
+    if len(lengths):
+        b = np.minimum(np.where(lengths > 0, np.floor(np.log2(np.maximum(lengths, 1))) + 1, 0),
+                       NBINS - 1).astype(int)
+        np.add.at(h, b, 1.0)
+        h /= len(lengths)
+    return h
+
+
+def features(tree, np_, ppb, n):
+    depth = tree.array("depth")
+    tag = tree.array("tag")
+    src_num = tree.array("src_num").astype(np.float64)
+    trg_num = tree.array("trg_num").astype(np.float64)
+    child = tree.array("child")
+    levels = np.bincount(np.minimum(depth, NLEVELS - 1), minlength=NLEVELS)[:NLEVELS]
+    f = [math.log(n), math.log(ppb), float(np_)]
+    f += list(np.log1p(levels))
+    trg_nodes = np.where(tag & 2)[0]
+    totals = []
+    for name in ("u", "v", "w", "x"):
+        ptr = tree.array(name + "_ptr")
+        idx = tree.array(name + "_idx")
+        lens = (ptr[1:] - ptr[:-1])[trg_nodes]
+        f += list(_hist(lens))
+        if name == "u":
+            # point pairs: targets of each leaf times the sources of its U list
+            per = np.zeros(len(ptr) - 1)
+            if len(idx):
+                cs = np.concatenate([[0.0], np.cumsum(src_num[idx])])
+                per = cs[ptr[1:]] - cs[ptr[:-1]]
+            leaves = child == -1
+            totals.append(float((trg_num * per)[leaves].sum()))
+        else:
+            totals.append(float(len(idx)))
+    f += [math.log1p(t) for t in totals]
+    # direct cost proxies: near-field pairs with the warp's 32-target
+    # granularity, boxes, leaves, boxes with a V list
+    leaves = child == -1
+    ptr = tree.array("u_ptr")
+    idx = tree.array("u_idx")
+    per = np.zeros(len(ptr) - 1)
+    if len(idx):
+        cs = np.concatenate([[0.0], np.cumsum(src_num[idx])])
+        per = cs[ptr[1:]] - cs[ptr[:-1]]
+    padded = float((np.ceil(trg_num / 32.0) * 32.0 * per)[leaves].sum())
+    vptr = tree.array("v_ptr")
+    f += [math.log1p(padded), math.log1p(len(depth)), math.log1p(float(np.sum(leaves & (src_num > 0)))),
+          math.log1p(float(np.sum(vptr[1:] > vptr[:-1])))]
+    return np.array(f, np.float64)
+
+
+def measure(K, pts, np_, ppb, precision, reps=2, device_tree=True):
+    """Per-phase device ms (minimum over reps after a warm-up) and the tree's
+    features."""
+    args = [pts[k] for k in ("sx", "sy", "sz", "tx", "ty", "tz")]
+    tree = K.Tree(*args, ppb, device=device_tree)
+    feats = features(tree, np_, ppb, len(pts["sx"]))
+    plan = K.Plan(tree, np_, precision)
+    try:
+        plan.set_points(pts)
+        plan.run()
+        plan.enable_timing(True)
+        best = None
+        for _ in range(reps):
+            plan.run()
+            ph = plan.phase_times()
+            v = np.array([ph[p] for p in PHASES])
+            best = v if best is None else np.minimum(best, v)
+        best[PHASES.index("down")] += ph["copy"]
+        return feats, best
+    finally:
+        plan.close()
+        tree.close()
+
+
+def cloud_specs(count, nmin=65536, nmax=1048576, seed=5):
+    rng = np.random.default_rng(seed)
+    kinds = ("uniform", "ellipsoidSurface", "clusters")
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
+        out.append({"kind": kinds[i % 3], "n": n, "seed": seed * 1000 + i})
+    return out
+
+
+def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, log=None):
+    """Measured dataset: one row per (cloud, leaf size)."""
+    precision = K.MIXED if precision is None else precision
+    rows_f, rows_t, cloud, ppbs = [], [], [], []
+    for ci, sp in enumerate(specs):
+        pts = make_cloud(K, sp["kind"], sp["n"], sp["seed"])
+        for ppb in leaf_sizes:
+            if ppb * 8 > sp["n"]:
+                continue
+            f, t = measure(K, pts, np_, ppb, precision)
+            rows_f.append(f)
+            rows_t.append(t)
+            cloud.append(ci)
+            ppbs.append(ppb)
+        if log:
+            log(f"cloud {ci} {sp['kind']} n={sp['n']}: done")
+    return {"features": np.array(rows_f), "phase_ms": np.array(rows_t), "cloud": np.array(cloud),
+            "ppb": np.array(ppbs), "n": np.array([specs[c]["n"] for c in cloud]),
+            "kind": np.array([specs[c]["kind"] for c in cloud])}
+
+
+class CostModel:
+    """Feature standardisation + the network; predicts per-phase log ms."""
+
+    def __init__(self, K, mean=None, std=None, params=None, hidden=64, seed=0):
+        self.K = K
+        self.mean, self.std = mean, std
+        self.hidden = hidden
+        self.net = None
+        if mean is not None:
+            self.net = K.MLP(len(mean), hidden, len(PHASES), params=params, seed=seed)
+
+    def _x(self, feats):
+        return ((np.atleast_2d(feats) - self.mean) / self.std).astype(np.float32)
+
+    def fit(self, feats, phase_ms, steps=4000, lr=2e-3, seed=0):
+        self.mean = feats.mean(0)
+        self.std = np.where(feats.std(0) > 1e-9, feats.std(0), 1.0)
+        self.net = self.K.MLP(feats.shape[1], self.hidden, len(PHASES), seed=seed)
+        T = np.log(np.maximum(phase_ms, 1e-3)).astype(np.float32)
+        return self.net.train(self._x(feats), T, steps, lr)
+
+    def predict_phase_ms(self, feats):
+        return np.exp(self.net.forward(self._x(feats)))
+
+    def predict_ms(self, feats):
+        return self.predict_phase_ms(feats).sum(1)
+
+    def save(self, path):
+        np.savez(path, mean=self.mean, std=self.std, params=self.net.params,
+                 hidden=self.hidden)
+
+    @classmethod
+    def load_default(cls, K):
+        """The network trained on the committed B200 harvest (NP=6, mixed)."""
+        return cls.load(K, os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                        "costmodel_data", "weights_b200_np6_mixed.npz"))
+
+    @classmethod
+    def load(cls, K, path):
+        z = np.load(path)
+        return cls(K, z["mean"], z["std"], z["params"], int(z["hidden"]))
+
+    def pick(self, pts, np_=6, precision=None, leaf_sizes=LEAF_SIZES, fallback_margin=0.10):
+        """(leaf size, {leaf size: predicted ms}, measured?) for a cloud."""
+        K = self.K
+        precision = K.MIXED if precision is None else precision
+        n = len(pts["sx"])
+        args = [pts[k] for k in ("sx", "sy", "sz", "tx", "ty", "tz")]
+        cand = [b for b in leaf_sizes if b * 8 <= n] or [leaf_sizes[0]]
+        feats = []
+        for ppb in cand:
+            tree = K.Tree(*args, ppb, device=True)
+            feats.append(features(tree, np_, ppb, n))
+            tree.close()
+        pred = dict(zip(cand, self.predict_ms(np.array(feats))))
+        order = sorted(cand, key=pred.get)
+        if len(order) > 1 and pred[order[1]] - pred[order[0]] < fallback_margin * pred[order[0]]:
+            from . import autotune
+            ms = {b: autotune.time_leaf_size(K, pts, b, np_, precision) for b in order[:2]}
+            return min(ms, key=ms.get), pred, True
+        return order[0], pred, False
+
+
+def evaluate_picks(model, data, clouds, default_ppb=512, fallback_margin=0.10):
+    """For each cloud of the dataset, from the harvested measurements: the
+    time of the model's pick, of the model with the measured fallback (the
+    two best predictions measured when they are within fallback_margin), of
+    the fixed default and of the sweep's best.  Ratios to the best."""
+    out = []
+    for c in clouds:
+        m = data["cloud"] == c
+        ppb = data["ppb"][m]
+        total = data["phase_ms"][m].sum(1)
+        pred = model.predict_ms(data["features"][m])
+        best = total.min()
+        order = np.argsort(pred)
+        pick = order[0]
+        fb = pick
+        measured = len(order) > 1 and pred[order[1]] - pred[order[0]] < fallback_margin * pred[order[0]]
+        if measured:
+            fb = order[:2][np.argmin(total[order[:2]])]
+        dflt = total[ppb == default_ppb][0] if np.any(ppb == default_ppb) else total[-1]
+        out.append({"cloud": int(c), "kind": str(data["kind"][m][0]), "n": int(data["n"][m][0]),
+                    "pick_over_best": float(total[pick] / best),
+                    "fallback_over_best": float(total[fb] / best), "measured": bool(measured),
+                    "default_over_best": float(dflt / best),
+                    "picked": int(ppb[pick]), "best": int(ppb[np.argmin(total)])})
+    return out
+
+
+def main(argv):
+    """harvest <out.npz> <nclouds>  |  train <data.npz> <weights.npz> [steps]"""
+    import __graft_entry__
+    K = __graft_entry__.load_package()
+    if argv[0] == "harvest":
+        specs = cloud_specs(int(argv[2]))
+        data = harvest(K, specs, log=print)
+        np.savez_compressed(argv[1], **data)
+    elif argv[0] == "train":
+        data = dict(np.load(argv[1]))
+        train = data["cloud"] % 5 != 0  # every fifth cloud held out
+        model = CostModel(K)
+        losses = model.fit(data["features"][train], data["phase_ms"][train],
+                           steps=int(argv[3]) if len(argv) > 3 else 4000)
+        model.save(argv[2])
+        held = sorted(set(data["cloud"][~train].tolist()))
+        ev = evaluate_picks(model, data, held)
+        print(json.dumps({"final_loss": float(losses[-1]), "held_out": ev}))
