@@ -13,9 +13,11 @@ sweep (autotune.best_leaf_size) the judge the model is scored against.
 Features of a (cloud, leaf size) tree: log point count, log leaf size, NP,
 node counts per level (16 levels), histograms of the U, V, W and X list
 lengths over target nodes (8 log2 bins each, as fractions), the log totals
-of U-list point pairs and V, W, X box pairs, and the logs of the near-field
-pairs padded to the kernel's 32-target granularity, of the box, leaf and
-V-list-box counts.  Targets: log(ms) of the
+of U-list point pairs and V, W, X box pairs, and the logs of the work the
+kernels do as the plan counts it: near-field pairs (U + W + direct X + L2T),
+the same padded to the warp's 32-target granularity, S2M and S2L pairs, the
+box, leaf and V-list-box counts, the largest leaf's near-field work and the
+work-weighted histogram of leaf work (8 bins, factors of 4).  Targets: log(ms) of the
 phases up, vlist, xlist, down, ulist (kfmm_phase_times).
 
 Clouds (``make_cloud``): the uniform cube, the ellipsoid surface, and
@@ -101,19 +103,46 @@ def features(tree, np_, ppb, n):
         else:
             totals.append(float(len(idx)))
     f += [math.log1p(t) for t in totals]
-    # direct cost proxies: near-field pairs with the warp's 32-target
-    # granularity, boxes, leaves, boxes with a V list
+    # the work the kernels do, counted as the plan counts it: near-field
+    # pairs (U + W + direct X + L2T) and the same padded to the warp's
+    # 32-target granularity, S2M and S2L pairs, boxes, leaves, V-list boxes
+    P = np_ ** 3 - (np_ - 2) ** 3
+    Q = (np_ + 2) ** 3 - np_ ** 3
+    nn = len(depth)
     leaves = child == -1
-    ptr = tree.array("u_ptr")
-    idx = tree.array("u_idx")
-    per = np.zeros(len(ptr) - 1)
-    if len(idx):
-        cs = np.concatenate([[0.0], np.cumsum(src_num[idx])])
-        per = cs[ptr[1:]] - cs[ptr[:-1]]
-    padded = float((np.ceil(trg_num / 32.0) * 32.0 * per)[leaves].sum())
+
+    def per_node(name, contrib):
+        ptr = tree.array(name + "_ptr")
+        idx = tree.array(name + "_idx")
+        if not len(idx):
+            return np.zeros(nn)
+        cs = np.concatenate([[0.0], np.cumsum(contrib(idx))])
+        return cs[ptr[1:]] - cs[ptr[:-1]]
+
+    src_leaf = leaves & (src_num > 0)
+    u = per_node("u", lambda i: src_num[i])
+    w = per_node("w", lambda i: np.where(src_leaf[i] & (src_num[i] < P), src_num[i], P))
+    x = per_node("x", lambda i: src_num[i])
+    near = u + w + np.where(trg_num < P, x, 0.0) + np.where(depth >= 2, P, 0.0)
+    tl = leaves & (trg_num > 0)
+    nf = float((trg_num * near)[tl].sum())
+    nf_pad = float((np.ceil(trg_num / 32.0) * 32.0 * near)[tl].sum())
+    s2m = float(Q * src_num[src_leaf].sum())
+    s2l = float((P * x)[(tag & 2).astype(bool) & ~(leaves & (trg_num < P))].sum())
     vptr = tree.array("v_ptr")
-    f += [math.log1p(padded), math.log1p(len(depth)), math.log1p(float(np.sum(leaves & (src_num > 0)))),
-          math.log1p(float(np.sum(vptr[1:] > vptr[:-1])))]
+    f += [math.log1p(v) for v in (nf, nf_pad, s2m, s2l, nn, float(src_leaf.sum()),
+                                  float(np.sum(vptr[1:] > vptr[:-1])))]
+    # how the near-field work is spread over the leaves (the persistent
+    # kernel's tail): largest leaf, and the work-weighted histogram of leaf
+    # work in factors of 4
+    lw = (np.ceil(trg_num / 32.0) * 32.0 * near)[tl]
+    f.append(math.log1p(float(lw.max()) if len(lw) else 0.0))
+    h = np.zeros(NBINS)
+    if len(lw) and lw.sum() > 0:
+        b = np.clip(np.floor(np.log(np.maximum(lw, 1.0) / 1e4) / np.log(4.0)) + 2, 0,
+                    NBINS - 1).astype(int)
+        np.add.at(h, b, lw / lw.sum())
+    f += list(h)
     return np.array(f, np.float64)
 
 

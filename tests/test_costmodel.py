@@ -54,7 +54,7 @@ def test_features_and_clusters(K):
         assert np.all(pts[k] >= -1) and np.all(pts[k] < 1)
     tree = K.Tree(*[pts[k] for k in ("sx", "sy", "sz", "tx", "ty", "tz")], 64)
     f = costmodel.features(tree, 6, 64, 20000)
-    assert f.shape == (3 + costmodel.NLEVELS + 4 * costmodel.NBINS + 8,)
+    assert f.shape == (3 + costmodel.NLEVELS + 5 * costmodel.NBINS + 12,)
     assert np.all(np.isfinite(f))
 
 
@@ -104,3 +104,19 @@ def test_model_picks_near_sweep_best(K, cuda_ok):
     assert pick <= 1.05
     assert fb <= pick
     assert pick < dflt
+
+
+@pytest.mark.gpu
+def test_work_features_equal_plan_counts(K, cuda_ok):
+    """The features' near-field, S2M and S2L pair counts are the plan's."""
+    from kifmm_b200 import costmodel
+    for kind, n, ppb, np_ in (("clusters", 40000, 32, 6), ("ellipsoidSurface", 30000, 48, 4)):
+        pts = costmodel.make_cloud(K, kind, n, 11)
+        tree = K.Tree(*[pts[k] for k in ("sx", "sy", "sz", "tx", "ty", "tz")], ppb, device=True)
+        f = costmodel.features(tree, np_, ppb, n)
+        base = 3 + costmodel.NLEVELS + 4 * costmodel.NBINS + 4
+        nf, _, s2m, s2l = np.expm1(f[base:base + 4])
+        st = K.Plan(tree, np_, K.MIXED).stats()
+        assert np.isclose(nf, st["u_pairs"], rtol=1e-12), (nf, st["u_pairs"])
+        assert np.isclose(s2m, st["s2m_pairs"], rtol=1e-12)
+        assert np.isclose(s2l, st["s2l_pairs"], rtol=1e-12, atol=0.5)
