@@ -115,6 +115,10 @@ struct kfmm_plan {
   bool timing = false;
   cudaEvent_t ev[7] = {};
   float phase_ms[6] = {};
+  // kfmm_evaluate uploads the targets on a second stream while the far field
+  // (which needs only the sources) runs
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_done = nullptr, src_done = nullptr;
 };
 
 namespace {
@@ -300,7 +304,7 @@ kfmm_status validate_desc(const kfmm_tree_desc* d) {
   return KFMM_OK;
 }
 
-// Key of a position within one level (coordinates < 2^20 since depth <= 20).
+// Key of a position within one level (coordinates < 2^21: plans accept depth <= 21).
 inline long long key_of(int x, int y, int z) {
   return (long long)x | ((long long)y << 21) | ((long long)z << 42);
 }
@@ -340,6 +344,10 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   int maxd = 0;
   for (int i = 0; i < nn; ++i) maxd = std::max(maxd, d->depth[i]);
   p->maxdepth = maxd;
+  if (maxd > 21) {  // key_of packs 21 bits per coordinate
+    set_error("kfmm_plan_create: trees deeper than 21 levels are not supported");
+    return KFMM_ERR_UNSUPPORTED;
+  }
 
   // --- tree arrays
   std::vector<double4> ctr(nn);
@@ -770,6 +778,9 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
                       (p->n_ifft > 0) + (p->n_s2l > 0) +
                       (int)p->down_gemms.size() + (p->n_nf > 0) + 1;
   for (int i = 0; i < 7; ++i) KF_CUDA(cudaEventCreate(&p->ev[i]));
+  KF_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
+  KF_CUDA(cudaEventCreateWithFlags(&p->side_done, cudaEventDisableTiming));
+  KF_CUDA(cudaEventCreateWithFlags(&p->src_done, cudaEventDisableTiming));
   return KFMM_OK;
 }
 
@@ -869,6 +880,9 @@ kfmm_status kfmm_plan_destroy(kfmm_plan* p) {
   for (void* v : p->allocs) cudaFree(v);
   for (int i = 0; i < 7; ++i)
     if (p->ev[i]) cudaEventDestroy(p->ev[i]);
+  if (p->side_done) cudaEventDestroy(p->side_done);
+  if (p->src_done) cudaEventDestroy(p->src_done);
+  if (p->side) cudaStreamDestroy(p->side);
   delete p;
   return KFMM_OK;
 }
@@ -1069,12 +1083,38 @@ kfmm_status kfmm_evaluate(kfmm_plan* p, const double* sx, const double* sy, cons
     set_error("kfmm_evaluate: null argument");
     return KFMM_ERR_INVALID;
   }
-  KF_TRY(kfmm_set_targets(p, tx, ty, tz, stream));
+  if (!tx || !ty || !tz) {
+    set_error("kfmm_evaluate: null argument");
+    return KFMM_ERR_INVALID;
+  }
+  // Sources first; the far field (up, V, X, down) needs nothing else, so it
+  // is queued on `stream` and the targets are uploaded and gathered on the
+  // plan's side stream meanwhile (after the sources' copy); the near field
+  // waits for them.  With pageable host arrays the target copy blocks this
+  // thread while the queued far field runs.
+  cudaStream_t st = S(stream);
   KF_TRY(kfmm_set_sources(p, sx, sy, sz, den, stream));
-  KF_TRY(kfmm_run(p, stream));
-  KF_CUDA(cudaMemcpyAsync(pot, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToHost,
-                          S(stream)));
-  KF_CUDA(cudaStreamSynchronize(S(stream)));
+  // the target copy starts once the sources are in (one transfer at a time)
+  KF_CUDA(cudaEventRecord(p->src_done, st));
+  KF_CUDA(cudaStreamWaitEvent(p->side, p->src_done, 0));
+  mark(p, 0, st);
+  KF_TRY(kfmm_up_calc(p, stream));
+  mark(p, 1, st);
+  KF_TRY(kfmm_vlist_calc(p, stream));
+  mark(p, 2, st);
+  KF_TRY(kfmm_xlist_calc(p, stream));
+  mark(p, 3, st);
+  KF_TRY(kfmm_down_calc(p, stream));
+  mark(p, 4, st);
+  KF_TRY(kfmm_set_targets(p, tx, ty, tz, p->side));
+  KF_CUDA(cudaEventRecord(p->side_done, p->side));
+  KF_CUDA(cudaStreamWaitEvent(st, p->side_done, 0));
+  KF_TRY(kfmm_ulist_calc(p, stream));
+  mark(p, 5, st);
+  KF_TRY(kfmm_copy_trg_val(p, nullptr, stream));
+  mark(p, 6, st);
+  KF_CUDA(cudaMemcpyAsync(pot, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToHost, st));
+  KF_CUDA(cudaStreamSynchronize(st));
   return KFMM_OK;
 }
 

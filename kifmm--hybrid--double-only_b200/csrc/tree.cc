@@ -147,6 +147,9 @@ void split_octants(const double* x, const double* y, const double* z, int* perm,
 
 }  // namespace
 
+constexpr int kMaxHostDepth = 30;
+struct TooDeep {};
+
 static void build_tree(Tree& T, int ns, const double* sx, const double* sy, const double* sz,
                        int nt, const double* tx, const double* ty, const double* tz,
                        int pts_max) {
@@ -167,6 +170,10 @@ static void build_tree(Tree& T, int ns, const double* sx, const double* sy, cons
   while (beg < end) {
     for (int k = beg; k < end; ++k) {
       if (re[k] - rb[k] <= pts_max) continue;
+      // more than pts_max coincident points never separate: the reference
+      // splits forever; here the depth is capped where the integer box
+      // coordinates would overflow
+      if (T.depth[k] >= kMaxHostDepth) throw TooDeep();
       int first = (int)T.parent.size();
       T.child[k] = first;
       for (int a = 0; a < 2; ++a)
@@ -387,6 +394,11 @@ extern "C" kfmm_status kfmm_tree_build(int num_src, const double* sx, const doub
     delete t;
     set_error("kfmm_tree_build: out of host memory");
     return KFMM_ERR_ALLOC;
+  } catch (const TooDeep&) {
+    delete t;
+    set_error("kfmm_tree_build: more than pts_max coincident sources: the tree would need more "
+              "than 30 levels");
+    return KFMM_ERR_UNSUPPORTED;
   }
   *out = t;
   return KFMM_OK;

@@ -95,3 +95,12 @@ def test_null_plan_calls(K):
     assert L.kfmm_run(None, None) == 1
     assert L.kfmm_plan_destroy(None) == 0
     assert L.kfmm_read_array(None, 0, None, 0) == 1
+
+
+def test_tree_build_refuses_coincident_overflow(K):
+    """More than pts_max coincident sources never separate: the reference's
+    builder splits forever; this one stops at 30 levels with an error."""
+    import numpy as np
+    x = np.full(50, 0.25)
+    with pytest.raises(K.KfmmError, match="coincident"):
+        K.Tree(x, x, x, x, x, x, 10)
