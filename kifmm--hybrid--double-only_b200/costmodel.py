@@ -8,7 +8,7 @@ no plan, no solve), the network predicts each candidate's time, and the
 fastest prediction wins.  When the two best predictions are closer than
 `fallback_margin` (10%), those two candidates are measured and the faster
 one is taken: measurement stays the fallback, and the exhaustive measured
-sweep (autotune.best_leaf_size) the judge the model is scored against.
+sweep (autotune.best_leaf_size) the yardstick the model is scored against.
 
 Features of a (cloud, leaf size) tree: log point count, log leaf size, NP,
 node counts per level (16 levels), histograms of the U, V, W and X list

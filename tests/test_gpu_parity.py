@@ -167,7 +167,7 @@ MIXED_CASES = [("uniform", 65536, 128, 6, 0), ("uniform", 60000, 64, 4, 1),
 @pytest.mark.parametrize("case", MIXED_CASES, ids=_ids)
 def test_mixed_precision_accuracy(K, oracle_mod, cuda_ok, case):
     """The mixed form (FP32 + compensated sums, FP64 final accumulation) is
-    judged by the reference's own check, the relative L2 error against an
+    measured by the reference's own check, the relative L2 error against an
     exact FP64 direct sum on sampled targets: it must stay within 2x the
     plain FP64 path's error; its distance to the plain path is reported."""
     dist, n, ppb, np_, coincide = case
@@ -212,3 +212,23 @@ def test_mixed_downward_check_vs_plain(K, cuda_ok, case):
     e = _node_err(out[K.MIXED], out[K.PLAIN_FP64], P, nodes)
     print(f"{_ids(case)}: mixed vs plain downward check potentials {e:.2e} over {len(nodes)} nodes")
     assert len(nodes) > 0 and e <= 2e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 2, 9, 100, 700])
+def test_tiny_inputs(K, oracle_mod, cuda_ok, n):
+    """Trees of a single leaf up to two levels: both forms against the oracle
+    and, for the plain form, the exact direct sum."""
+    pts = K.generate_points(n, "uniform", 0, 26)
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], 8)
+    tarrs = {k: tree.array(k) for k in oracle_mod.TREE_FIELDS}
+    ref = oracle_mod.evaluate(tarrs, 4, K.operators(4), pts)
+    plain = K.Plan(tree, 4, K.PLAIN_FP64).evaluate(pts)
+    mixed = K.Plan(tree, 4, K.MIXED).evaluate(pts)
+    assert np.all(np.isfinite(plain)) and np.all(np.isfinite(mixed))
+    assert np.max(np.abs(plain - ref) / np.abs(ref)) <= 1e-12
+    assert np.max(np.abs(mixed - ref) / np.abs(ref)) <= 1e-5
+    if tree.desc.num_nodes == 1:
+        d = oracle_mod.direct(pts["tx"], pts["ty"], pts["tz"], pts["sx"], pts["sy"], pts["sz"],
+                              pts["den"])
+        assert np.max(np.abs(plain - d) / np.abs(d)) <= 1e-13
