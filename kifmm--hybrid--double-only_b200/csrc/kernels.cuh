@@ -626,8 +626,10 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
   __shared__ double2 X[B][NP * NP * NK];
   __shared__ double2 Y[B][NP * N * NK];
   __shared__ double cs[N], sn[N];
+  constexpr int P = NP * NP * NP - (NP - 2) * (NP - 2) * (NP - 2);
   __shared__ int node_s[B];
   __shared__ double scale_s[B];
+  __shared__ int cell_s[P];  // surface point -> cell of the np^3 block
   const int tid = threadIdx.x;
   const int b0 = blockIdx.x * B;
   if (tid < N) {
@@ -639,12 +641,16 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
     node_s[tid] = node;
     scale_s[tid] = node >= 0 ? ldexp(1.0, p.depth[node]) : 0.0;
   }
+  for (int q = tid; q < P; q += kFFTThreads)
+    cell_s[q] = (p.surf_ijk[3 * q] * NP + p.surf_ijk[3 * q + 1]) * NP + p.surf_ijk[3 * q + 2];
+  for (int q = tid; q < B * NP * NP * NP; q += kFFTThreads) (&den[0][0])[q] = 0.0;
   __syncthreads();
-  for (int q = tid; q < B * NP * NP * NP; q += kFFTThreads) {
-    const int bb = q / (NP * NP * NP), r = q % (NP * NP * NP);
+  // the P surface values of each box: consecutive threads read consecutive
+  // values and scatter them into the box's np^3 block
+  for (int q = tid; q < B * P; q += kFFTThreads) {
+    const int bb = q / P, s = q % P;
     const int node = node_s[bb];
-    const int sidx = p.surf_idx[r];
-    den[bb][r] = (node >= 0 && sidx >= 0) ? p.pln[(size_t)node * p.P + sidx] * scale_s[bb] : 0.0;
+    if (node >= 0) den[bb][cell_s[s]] = p.pln[(size_t)node * p.P + s] * scale_s[bb];
   }
   __syncthreads();
   // x: row (k = z, j = y), outputs kx
