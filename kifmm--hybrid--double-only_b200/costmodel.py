@@ -198,7 +198,8 @@ def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, log=None):
             log(f"cloud {ci} {sp['kind']} n={sp['n']}: done")
     return {"features": np.array(rows_f), "phase_ms": np.array(rows_t), "cloud": np.array(cloud),
             "ppb": np.array(ppbs), "n": np.array([specs[c]["n"] for c in cloud]),
-            "kind": np.array([specs[c]["kind"] for c in cloud])}
+            "kind": np.array([specs[c]["kind"] for c in cloud]),
+            "seed": np.array([specs[c]["seed"] for c in cloud])}
 
 
 class CostModel:

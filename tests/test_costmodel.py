@@ -7,7 +7,7 @@
 * Full-batch training on the GPU (kfmm_mlp_train) fits a smooth synthetic
   regression.
 * With the dataset harvested on a B200 (per-phase times of 6 leaf sizes for
-  400 clouds of 65,536 to 1,048,576 uniform, ellipsoid-surface and
+  430 clouds of 65,536 to 4,194,304 uniform, ellipsoid-surface and
   Gaussian-cluster points, NP=6, mixed form) and the network trained on the
   GPU on four fifths of its clouds, the model's pick on the held-out clouds
   runs within 5% of the measured sweep's best on average, the measured
