@@ -385,6 +385,24 @@ __device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, in
   }
 }
 
+template <bool kMixed>
+__device__ __forceinline__ void run_job(const P2PParams& p, const P2PJob& J, int lane, void* wb) {
+  switch ((J.tcnt + 31) >> 5) {
+    case 1: warp_job<kMixed, 1>(p, J, lane, wb); break;
+    case 2: warp_job<kMixed, 2>(p, J, lane, wb); break;
+    case 3: warp_job<kMixed, 3>(p, J, lane, wb); break;
+    case 4: warp_job<kMixed, 4>(p, J, lane, wb); break;
+    case 5: warp_job<kMixed, 5>(p, J, lane, wb); break;
+    default: warp_job<kMixed, kMaxSlots>(p, J, lane, wb); break;
+  }
+}
+
+__device__ __forceinline__ int next_job_of_warp(int* next_job, int lane) {
+  int j = 0;
+  if (lane == 0) j = atomicAdd(next_job, 1);
+  return __shfl_sync(0xffffffffu, j, 0);
+}
+
 // Persistent: each warp takes jobs from *next_job until none are left.  The
 // counter is zeroed on the stream before every launch.
 template <bool kMixed>
@@ -407,6 +425,24 @@ p2p_warp_kernel(P2PParams p, int njobs, int* next_job) {
       case 5: warp_job<kMixed, 5>(p, J, lane, wb); break;
       default: warp_job<kMixed, kMaxSlots>(p, J, lane, wb); break;
     }
+  }
+}
+
+// The near fields of many plans in one persistent launch (batched solves):
+// job j is job jobs[j].y of plan jobs[j].x, whose arrays params[jobs[j].x]
+// describes.
+template <bool kMixed>
+__global__ void __launch_bounds__(32 * kWarpJobsPerBlock, kMixed ? KFMM_P2P_MIXED_MINB : 4)
+p2p_fused_kernel(const P2PParams* params, const int2* jobs, int njobs, int* next_job) {
+  __shared__ __align__(16) unsigned char smem[kWarpJobsPerBlock][32 * 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  void* wb = smem[wid];
+  for (;;) {
+    const int j = next_job_of_warp(next_job, lane);
+    if (j >= njobs) return;
+    const int2 pj = jobs[j];
+    const P2PParams& p = params[pj.x];
+    run_job<kMixed>(p, p.jobs[pj.y], lane, wb);
   }
 }
 

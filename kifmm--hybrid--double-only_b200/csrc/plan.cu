@@ -94,6 +94,7 @@ struct kfmm_plan {
   P2PJob *s2m_jobs = nullptr, *nf_jobs = nullptr, *s2l_jobs = nullptr;
   int *s2m_ent = nullptr, *nf_ent = nullptr, *s2l_ent = nullptr;
   int n_s2m = 0, n_nf = 0, n_s2l = 0;
+  std::vector<float> nf_class;  // cost class of each near-field job (-log1.25 cost)
   int* job_counter = nullptr;  // persistent P2P work counters: S2M, S2L, near field
   int* d_error = nullptr;      // set by kernels whose bounded waits ran out
   int had32_groups_per_block = 0;
@@ -480,7 +481,8 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   // x sources, in classes 25% wide); within a class the jobs keep their tree
   // order, so warps working at the same time read neighbouring leaves' sources
   // and the L2 cache serves the repeats.
-  auto order_jobs = [&](std::vector<P2PJob>& jobs, const std::vector<int>& ent) {
+  auto order_jobs = [&](std::vector<P2PJob>& jobs, const std::vector<int>& ent,
+                        std::vector<float>* class_out = nullptr) {
     std::vector<std::pair<double, int>> key(jobs.size());
     for (size_t j = 0; j < jobs.size(); ++j) {
       double ns = 0;
@@ -495,6 +497,10 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     std::vector<P2PJob> out(jobs.size());
     for (size_t j = 0; j < jobs.size(); ++j) out[j] = jobs[key[j].second];
     jobs.swap(out);
+    if (class_out) {
+      class_out->resize(jobs.size());
+      for (size_t j = 0; j < jobs.size(); ++j) (*class_out)[j] = (float)key[j].first;
+    }
   };
 
   // --- up: S2M jobs + UC2UE GEMM, then M2M per level
@@ -726,7 +732,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       add_chunks(jobs, t, 0, d->trg_beg[t], d->trg_num[t], e0, (int)ent.size(), d->trg_beg[t], 0);
       p->stats.u_pairs += (double)d->trg_num[t] * ns;
     }
-    order_jobs(jobs, ent);
+    order_jobs(jobs, ent, &p->nf_class);
     p->n_nf = (int)jobs.size();
     KF_TRY(upload(p, &p->nf_jobs, jobs));
     KF_TRY(upload(p, &p->nf_ent, ent));
@@ -1050,15 +1056,11 @@ kfmm_status kfmm_get_potentials_device(kfmm_plan* p, double* pot_dev, void* stre
   return KFMM_OK;
 }
 
-kfmm_status kfmm_run(kfmm_plan* p, void* stream) {
-  if (!p) {
-    set_error("kfmm_run: null plan");
-    return KFMM_ERR_INVALID;
-  }
-  if (!p->have_src || !p->have_trg) {
-    set_error("kfmm_run: set sources and targets first");
-    return KFMM_ERR_STATE;
-  }
+}  // extern "C"
+
+namespace {
+// up, V, X (S2L) and down: everything before the near field
+kfmm_status run_far_field(kfmm_plan* p, void* stream) {
   cudaStream_t st = S(stream);
   mark(p, 0, st);
   KF_TRY(kfmm_up_calc(p, stream));
@@ -1069,10 +1071,26 @@ kfmm_status kfmm_run(kfmm_plan* p, void* stream) {
   mark(p, 3, st);
   KF_TRY(kfmm_down_calc(p, stream));
   mark(p, 4, st);
+  return KFMM_OK;
+}
+}  // namespace
+
+extern "C" {
+
+kfmm_status kfmm_run(kfmm_plan* p, void* stream) {
+  if (!p) {
+    set_error("kfmm_run: null plan");
+    return KFMM_ERR_INVALID;
+  }
+  if (!p->have_src || !p->have_trg) {
+    set_error("kfmm_run: set sources and targets first");
+    return KFMM_ERR_STATE;
+  }
+  KF_TRY(run_far_field(p, stream));
   KF_TRY(kfmm_ulist_calc(p, stream));
-  mark(p, 5, st);
+  mark(p, 5, S(stream));
   KF_TRY(kfmm_copy_trg_val(p, nullptr, stream));
-  mark(p, 6, st);
+  mark(p, 6, S(stream));
   return KFMM_OK;
 }
 
@@ -1097,15 +1115,7 @@ kfmm_status kfmm_evaluate(kfmm_plan* p, const double* sx, const double* sy, cons
   // the target copy starts once the sources are in (one transfer at a time)
   KF_CUDA(cudaEventRecord(p->src_done, st));
   KF_CUDA(cudaStreamWaitEvent(p->side, p->src_done, 0));
-  mark(p, 0, st);
-  KF_TRY(kfmm_up_calc(p, stream));
-  mark(p, 1, st);
-  KF_TRY(kfmm_vlist_calc(p, stream));
-  mark(p, 2, st);
-  KF_TRY(kfmm_xlist_calc(p, stream));
-  mark(p, 3, st);
-  KF_TRY(kfmm_down_calc(p, stream));
-  mark(p, 4, st);
+  KF_TRY(run_far_field(p, stream));
   KF_TRY(kfmm_set_targets(p, tx, ty, tz, p->side));
   KF_CUDA(cudaEventRecord(p->side_done, p->side));
   KF_CUDA(cudaStreamWaitEvent(st, p->side_done, 0));
@@ -1174,12 +1184,20 @@ struct kfmm_batch {
   std::vector<cudaEvent_t> events;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // fused near field of all plans: per-plan kernel arguments, (plan, job)
+  // pairs in cost-class order, the job counter
+  P2PParams* d_params = nullptr;
+  int2* d_jobs = nullptr;
+  int* d_counter = nullptr;
 };
 
 static void batch_release(kfmm_batch* b) {
   if (!b) return;
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->d_params) cudaFree(b->d_params);
+  if (b->d_jobs) cudaFree(b->d_jobs);
+  if (b->d_counter) cudaFree(b->d_counter);
   for (cudaEvent_t e : b->events) cudaEventDestroy(e);
   for (cudaStream_t s : b->streams) cudaStreamDestroy(s);
   delete b;
@@ -1217,23 +1235,84 @@ kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
     if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
       return fail(e, "cudaEventCreate");
   }
+  // Plans of one precision share one near-field launch: their far fields run
+  // on the branch streams, then a single persistent launch takes the jobs of
+  // all plans, largest cost class first, so small solves do not leave SMs
+  // idle.
+  bool fused = true;
+  size_t njobs = 0;
+  for (int i = 0; i < nplans; ++i) {
+    fused = fused && plans[i]->prec == plans[0]->prec;
+    njobs += plans[i]->n_nf;
+  }
+  fused = fused && njobs > 0 && njobs < (size_t)INT32_MAX;
+  if (fused) {
+    std::vector<P2PParams> params(nplans);
+    std::vector<std::pair<float, int2>> order;
+    order.reserve(njobs);
+    for (int i = 0; i < nplans; ++i) {
+      kfmm_plan* p = plans[i];
+      params[i] = p2p_params(p, p->nf_jobs, p->nf_ent, p->pot_leaf);
+      for (int j = 0; j < p->n_nf; ++j) order.push_back({p->nf_class[j], make_int2(i, j)});
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [](const std::pair<float, int2>& a, const std::pair<float, int2>& c) {
+                       return a.first < c.first;
+                     });
+    std::vector<int2> jobs(njobs);
+    for (size_t j = 0; j < njobs; ++j) jobs[j] = order[j].second;
+    if ((e = cudaMalloc(&b->d_params, sizeof(P2PParams) * nplans)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_jobs, sizeof(int2) * njobs)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_counter, sizeof(int))) != cudaSuccess)
+      return fail(e, "cudaMalloc");
+    if ((e = cudaMemcpy(b->d_params, params.data(), sizeof(P2PParams) * nplans,
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(b->d_jobs, jobs.data(), sizeof(int2) * njobs, cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+      return fail(e, "cudaMemcpy");
+  }
   cudaStream_t origin = b->streams[nstreams];
   if ((e = cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
     return fail(e, "cudaStreamBeginCapture");
   // fork: every branch stream waits on the origin, then runs its plans
-  cudaEventRecord(b->events[nstreams], origin);
-  for (int k = 0; k < nstreams; ++k) cudaStreamWaitEvent(b->streams[k], b->events[nstreams], 0);
+  auto fork = [&]() {
+    cudaEventRecord(b->events[nstreams], origin);
+    for (int k = 0; k < nstreams; ++k) cudaStreamWaitEvent(b->streams[k], b->events[nstreams], 0);
+  };
+  auto join = [&]() {
+    for (int k = 0; k < nstreams; ++k) {
+      cudaEventRecord(b->events[k], b->streams[k]);
+      cudaStreamWaitEvent(origin, b->events[k], 0);
+    }
+  };
+  fork();
   kfmm_status st = KFMM_OK;
   for (int i = 0; i < nplans && st == KFMM_OK; ++i) {
     const bool timing = plans[i]->timing;
     plans[i]->timing = false;
-    st = kfmm_run(plans[i], b->streams[i % nstreams]);
+    st = fused ? run_far_field(plans[i], b->streams[i % nstreams])
+               : kfmm_run(plans[i], b->streams[i % nstreams]);
     plans[i]->timing = timing;
   }
-  // join
-  for (int k = 0; k < nstreams; ++k) {
-    cudaEventRecord(b->events[k], b->streams[k]);
-    cudaStreamWaitEvent(origin, b->events[k], 0);
+  join();
+  if (fused && st == KFMM_OK) {
+    cudaMemsetAsync(b->d_counter, 0, sizeof(int), origin);
+    const int blocks = std::min(plans[0]->p2p_grid,
+                                (int)((njobs + kWarpJobsPerBlock - 1) / kWarpJobsPerBlock));
+    if (plans[0]->prec == KFMM_MIXED)
+      p2p_fused_kernel<true><<<blocks, 32 * kWarpJobsPerBlock, 0, origin>>>(
+          b->d_params, b->d_jobs, (int)njobs, b->d_counter);
+    else
+      p2p_fused_kernel<false><<<blocks, 32 * kWarpJobsPerBlock, 0, origin>>>(
+          b->d_params, b->d_jobs, (int)njobs, b->d_counter);
+    if (cudaGetLastError() != cudaSuccess) {
+      set_error("kfmm_batch_create: fused near-field launch failed");
+      st = KFMM_ERR_CUDA;
+    }
+    fork();
+    for (int i = 0; i < nplans && st == KFMM_OK; ++i)
+      st = kfmm_copy_trg_val(plans[i], nullptr, b->streams[i % nstreams]);
+    join();
   }
   e = cudaStreamEndCapture(origin, &b->graph);
   if (st != KFMM_OK) {
