@@ -250,7 +250,7 @@ def time_batched(K, count, stream, steps, warmup, dev):
     pots = {}
     for name, prec in (("mixed", K.MIXED), ("fp64", K.PLAIN_FP64)):
         table = autotune.LeafSizeTable()
-        B = batched.BatchedSolves(K, sp, prec, table=table, nstreams=8)
+        B = batched.BatchedSolves(K, sp, prec, table=table, nstreams=16)
         for _ in range(warmup):
             B.launch(sh)
         torch.cuda.synchronize()

@@ -294,7 +294,7 @@ class Batch:
     plans must have their points set; they stay owned by the caller and must
     outlive the batch."""
 
-    def __init__(self, plans, nstreams=8):
+    def __init__(self, plans, nstreams=16):
         self.plans = list(plans)
         arr = (ctypes.c_void_p * len(self.plans))(*[p.handle for p in self.plans])
         h = ctypes.c_void_p()

@@ -25,7 +25,7 @@ def specs(count, nmin=4096, nmax=262144, seed=2024):
 
 
 class BatchedSolves:
-    def __init__(self, K, solves, precision, table=None, nstreams=8, num_check=0):
+    def __init__(self, K, solves, precision, table=None, nstreams=16, num_check=0):
         self.K = K
         self.table = table if table is not None else autotune.LeafSizeTable()
         self.solves = []
