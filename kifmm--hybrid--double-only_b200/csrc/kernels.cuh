@@ -866,6 +866,16 @@ constexpr int kHadThreads = 256;  // 8 warps, one group per warp, lane = frequen
 constexpr int kHadGroupsInFlight = kHadThreads / 32;
 constexpr int kHadGroupsPerBlock = 32;
 
+// A row of the translation table at (dy, dz) with |dy| <= 1 and |dz| <= 1:
+// its entries dx = -1, 0, 1 (k = 2, 3, 4 of the row) are adjacent offsets,
+// whose spectra are zero (they are not V-list interactions), so the FP64
+// window kernel skips those loads and multiply-adds: 27 of the 216 per member.
+// (The FP32 kernels below are FMA-bound with their loads scheduled across the
+// rows; there a branch per row costs more than the skipped work.)
+__device__ __forceinline__ bool near_row(int dy, int dz) {
+  return dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1;
+}
+
 __device__ __forceinline__ void cmac64(double& ar, double& ai, const double2 t, const double2 s) {
   ar = fma(t.x, s.x, ar);
   ar = fma(-t.y, s.y, ar);
@@ -930,16 +940,24 @@ __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p)
         const double2* trow =
             p.trans + (size_t)((wz - 2 - cz + 3) * 49 + (wy - 2 - cy + 3) * 7) * p.Fpad +
             fb * kFB + f;
-        double2 t[7];
+        auto row_body = [&](auto near) {
+          constexpr bool kNear = decltype(near)::value;
+          double2 t[7];
 #pragma unroll
-        for (int k = 0; k < 7; ++k) t[k] = __ldg(trow + (size_t)k * p.Fpad);
+          for (int k = 0; k < 7; ++k)
+            t[k] = kNear && k >= 2 && k <= 4 ? make_double2(0.0, 0.0)
+                                            : __ldg(trow + (size_t)k * p.Fpad);
 #pragma unroll
-        for (int wx = 0; wx < 6; ++wx)
+          for (int wx = 0; wx < 6; ++wx)
 #pragma unroll
-          for (int cx = 0; cx < 2; ++cx) {
-            const int c = cx * 4 + cy * 2 + cz;
-            cmac64(ar[c], ai[c], t[wx - cx + 1], srow[wx]);
-          }
+            for (int cx = 0; cx < 2; ++cx) {
+              const int c = cx * 4 + cy * 2 + cz, k = wx - cx + 1;
+              if (kNear && k >= 2 && k <= 4) continue;
+              cmac64(ar[c], ai[c], t[k], srow[wx]);
+            }
+        };
+        if (near_row(wy - 2 - cy, wz - 2 - cz)) row_body(std::true_type{});
+        else row_body(std::false_type{});
       }
     }
 #pragma unroll
@@ -959,8 +977,9 @@ __global__ void __launch_bounds__(kHadThreads) hadamard_kernel(HadamardParams p)
 //   A += {tr, ti} * {sr, sr},  B += {tr, ti} * {si, si},
 //   re = A.x - B.y,  im = A.y + B.x
 // so a lane reads 8 B of shared memory per 12/7 multiply-adds and spends no
-// instruction on rearranging it.  The products of one z-plane of the window
-// (72 per member) are summed in FP32 and the plane sums accumulated in FP64.
+// instruction on rearranging it.  The products of each half of the window
+// (z-planes 0-2 and 3-5, 108 per member of which up to 27 are zero) are
+// summed in FP32 and the two half sums added in FP64.
 // Warps are autonomous: each loads its own group's window into its slice of
 // shared memory.
 constexpr int kHad32Threads = 512;
@@ -1100,7 +1119,7 @@ __global__ void __launch_bounds__(kHad32Threads, 1) hadamard_fp32_kernel(Had32Pa
                 : "l"(tk), "l"(sr[wx]), "l"(si[wx]));
           }
       }
-      if (wy == 5) {  // end of a z-plane of the window
+      if (row == 17 || row == 35) {  // end of z-planes 0-2 and 3-5 of the window
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
           ar[c] += (double)lo_of(A[c]) - (double)hi_of(B[c]);
@@ -1122,9 +1141,9 @@ __global__ void __launch_bounds__(kHad32Threads, 1) hadamard_fp32_kernel(Had32Pa
 // x + 1) share one 8 x 6 x 6 window: a row of 8 source spectra meets each
 // row of 7 translation values for both groups, 24 multiply-adds per 7 shared
 // loads, which halves the shared-memory traffic per multiply-add.  The 16
-// members' FP32 sums are flushed at the end of every z-plane into FP64 sums
-// kept in the warp's slice of shared memory.  12 warps per CTA (up to 168 registers a
-// thread).
+// members' FP32 sums of the first half-window are kept in FP64 in the warp's
+// slice of shared memory and added to the second half's at the end.  12 warps
+// per CTA (up to 168 registers a thread).
 constexpr int kHadPairThreads = 384;
 constexpr int kHadPairWarps = kHadPairThreads / 32;
 constexpr size_t kHadPairSumBytes = sizeof(double) * kHadPairWarps * 16 * 2 * 32;
@@ -1156,8 +1175,6 @@ __global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(
   for (int g = g0 + slot; g < g1; g += kHadPairWarps) {
     for (int q = f; q < 288; q += 32) win[slot][q] = p.win[(size_t)g * 288 + q];
     if (f < 16) mem[slot][f] = p.members[(size_t)g * 16 + f];
-#pragma unroll
-    for (int c = 0; c < 32; ++c) sums[c * 32] = 0.0;
     __syncwarp();
     const int* w = win[slot];
     unsigned long long nxt[8];
@@ -1207,11 +1224,11 @@ __global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(
                   : "l"(tk), "l"(sr[wx + 2 * h]), "l"(si[wx + 2 * h]));
             }
       }
-      if (wy == 5) {  // end of a z-plane of the window
+      if (row == 17) {  // end of z-planes 0-2: first half-window sums to FP64
 #pragma unroll
         for (int c = 0; c < 16; ++c) {
-          sums[(2 * c) * 32] += (double)lo_of(A[c]) - (double)hi_of(B[c]);
-          sums[(2 * c + 1) * 32] += (double)hi_of(A[c]) + (double)lo_of(B[c]);
+          sums[(2 * c) * 32] = (double)lo_of(A[c]) - (double)hi_of(B[c]);
+          sums[(2 * c + 1) * 32] = (double)hi_of(A[c]) + (double)lo_of(B[c]);
           A[c] = B[c] = 0ull;
         }
       }
@@ -1221,7 +1238,8 @@ __global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(
       const int m = mem[slot][c];
       if (m >= 0)
         p.effv[(fbase + m) * kFB + f] =
-            make_float2((float)sums[(2 * c) * 32], (float)sums[(2 * c + 1) * 32]);
+            make_float2((float)(sums[(2 * c) * 32] + ((double)lo_of(A[c]) - (double)hi_of(B[c]))),
+                        (float)(sums[(2 * c + 1) * 32] + ((double)hi_of(A[c]) + (double)lo_of(B[c]))));
     }
     __syncwarp();
   }

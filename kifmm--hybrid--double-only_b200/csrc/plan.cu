@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <unordered_map>
@@ -378,13 +379,19 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   }
   p->Fpad = (F + kFB - 1) / kFB * kFB;
   p->cplx = p->prec == KFMM_MIXED ? sizeof(float2) : sizeof(double2);
+  // Offsets with |delta|_inf <= 1 are adjacent boxes, never V-list pairs: the
+  // table keeps zeros there whatever the supplied operators hold, and the
+  // Hadamard kernels skip them.
+  auto adjacent = [](int id) {
+    return std::abs(id % 7 - 3) <= 1 && std::abs(id / 7 % 7 - 3) <= 1 && std::abs(id / 49 - 3) <= 1;
+  };
   if (p->prec == KFMM_MIXED) {
     // [fb][343][32]: one contiguous 87,808-byte tile per block of 32
     // frequencies (hadamard_fp32_kernel)
     const int nfb = p->Fpad / kFB;
     std::vector<float2> tr((size_t)nfb * 343 * kFB, make_float2(0.f, 0.f));
     for (int id = 0; id < 343; ++id)
-      for (int f = 0; f < F; ++f)
+      for (int f = 0; f < F && !adjacent(id); ++f)
         tr[((size_t)(f / kFB) * 343 + id) * kFB + f % kFB] =
             make_float2((float)op.ue2dc[2 * ((size_t)id * F + f)],
                         (float)op.ue2dc[2 * ((size_t)id * F + f) + 1]);
@@ -394,7 +401,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   } else {
     std::vector<double2> tr((size_t)343 * p->Fpad, make_double2(0.0, 0.0));
     for (int id = 0; id < 343; ++id)
-      for (int f = 0; f < F; ++f)
+      for (int f = 0; f < F && !adjacent(id); ++f)
         tr[(size_t)id * p->Fpad + f] = make_double2(op.ue2dc[2 * ((size_t)id * F + f)],
                                                     op.ue2dc[2 * ((size_t)id * F + f) + 1]);
     double2* d = nullptr;
