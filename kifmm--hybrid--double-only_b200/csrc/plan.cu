@@ -753,12 +753,23 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kHadPairSmemBytes));
   {
-    // about 8 waves of one CTA per SM over (chunks x frequency blocks)
+    // One CTA per SM over (chunks x frequency blocks).  A chunk holds k
+    // windows per warp (every warp the same count, so none idles at the end
+    // of its CTA); k minimises the span ceil(CTAs / SMs) x (k + 0.1), the 0.1
+    // standing for a CTA's translation-tile load.
     const int nfb = p->Fpad / kFB;
     auto per_block = [&](int items, int warps) {
-      const int max_chunks = std::max(1, (items + warps - 1) / warps);
-      const int chunks = std::max(1, std::min(max_chunks, (8 * p->num_sms + nfb - 1) / nfb));
-      return std::max(1, (items + chunks - 1) / chunks);
+      int pick = warps;
+      double best = 1e300;
+      for (int k = 1; k <= 8; ++k) {
+        const long long ctas = (long long)((items + warps * k - 1) / (warps * k)) * nfb;
+        const double span = std::ceil((double)ctas / p->num_sms) * (k + 0.1);
+        if (span < best) {
+          best = span;
+          pick = warps * k;
+        }
+      }
+      return pick;
     };
     p->had32_groups_per_block = per_block(p->n_singles, kHad32Warps);
     p->pair_per_block = per_block(p->n_pairs, kHadPairWarps);
