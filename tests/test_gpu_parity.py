@@ -159,6 +159,31 @@ def test_repeat_runs_identical(K, cuda_ok):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["plain", "mixed"])
+def test_adjacent_translation_spectra_ignored(K, cuda_ok, precision):
+    """Offsets with |delta|_inf <= 1 are adjacent boxes, never V-list pairs
+    (fmm/omp_sse_block.cc:581-593 visits V-list members only), and the window
+    kernels skip them: a supplied translation table with garbage there gives
+    the same potentials, bit for bit, as the plan's own table."""
+    prec = K.PLAIN_FP64 if precision == "plain" else K.MIXED
+    np_ = 4
+    pts = K.generate_points(20000, "ellipsoidSurface", 0, 11)
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], 32)
+    ops = K.operators(np_)
+    F = K.sizes(np_)[2]
+    bad = {k: v.copy() for k, v in ops.items()}
+    t = bad["ue2dc"].reshape(343, 2 * F)
+    rng = np.random.default_rng(5)
+    for i3 in (-1, 0, 1):
+        for i2 in (-1, 0, 1):
+            for i1 in (-1, 0, 1):
+                t[(i1 + 3) + 7 * (i2 + 3) + 49 * (i3 + 3)] = rng.normal(size=2 * F) * 1e3
+    a = K.Plan(tree, np_, prec, operators=ops).evaluate(pts)
+    b = K.Plan(tree, np_, prec, operators=bad).evaluate(pts)
+    assert np.array_equal(a, b)
+
+
 MIXED_CASES = [("uniform", 65536, 128, 6, 0), ("uniform", 60000, 64, 4, 1),
                ("ellipsoidSurface", 60000, 40, 4, 0), ("ellipseUniformAngles", 40000, 24, 5, 0)]
 
