@@ -55,6 +55,22 @@ struct P2PParams {
   int P, Q;
 };
 
+// The mixed form's kernels take these besides (a separate struct: the plain
+// form's kernel keeps its argument block, and ptxas its register allocation).
+struct P2PMixedParams {
+  P2PParams p;
+  // leaf-order sources as FP32 offsets from their leaf's centre with the
+  // density in FP32 (made once per upload); node centres in FP32
+  const float4* src4f;
+  const float4* ctrf;
+  const float* spf_ue;  // the unit UE / DE surfaces in FP32, 3 per point
+  const float* spf_de;
+};
+template <bool kMixed>
+using P2PArgs = typename std::conditional<kMixed, P2PMixedParams, P2PParams>::type;
+__device__ __forceinline__ const P2PParams& base_of(const P2PParams& a) { return a; }
+__device__ __forceinline__ const P2PParams& base_of(const P2PMixedParams& a) { return a.p; }
+
 __device__ __forceinline__ double3 surface_point(const double4 c, const double* sp, int k) {
   // centre + radius * unit-surface point, unfused as fmm/trans.cc:92-100
   double3 r;
@@ -65,10 +81,15 @@ __device__ __forceinline__ double3 surface_point(const double4 c, const double* 
 }
 
 // Mixed precision P2P (kMixed below): coordinates are taken relative to the
-// target set's own node centre in FP64 and then rounded to FP32, so the FP32
-// differences keep ~1e-7 of the box size; 1/r comes from the FP32 reciprocal
-// square root; terms are summed in FP32 over blocks of 16 sources and the
-// block sums in FP64; the result is scaled by 1/(4 pi) in FP64.
+// target set's own node centre and rounded to FP32, so the FP32 differences
+// keep ~1e-7 of the box size; 1/r comes from the FP32 reciprocal square root;
+// terms are summed in FP32 over blocks of 16 sources and the block sums in
+// FP64; the result is scaled by 1/(4 pi) in FP64.  Leaf sources are stored as
+// FP32 offsets from their own leaf's centre (src4f); the offset between the
+// leaf's and the target node's centres is exact in FP32 (centres are
+// -1 + (2i + 1) 2^-d: the difference of two is a multiple of 2^-20 below 2 in
+// magnitude for the depths <= 20 that plans accept), so a source costs one
+// FP32 rounding more than a direct conversion, and half the bytes.
 
 // ---------------------------------------------------------------------------
 // Warp-autonomous P2P.  One warp owns one job of up to 32*kMaxSlots targets
@@ -266,9 +287,129 @@ __device__ __forceinline__ void pairs_mixed(const unsigned long long (&tx)[(NS +
   }
 }
 
-template <bool kMixed, int NS>
-__device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, int lane,
-                                         void* wbuf) {
+// Target i of job J (i < J.tcnt), absolute FP64 coordinates.
+__device__ __forceinline__ double3 job_target(const P2PParams& p, const P2PJob& J,
+                                              const double4 org, int i) {
+  if (J.tkind == 0) {
+    const double4 w = p.trg4[J.tbeg + i];
+    return make_double3(w.x, w.y, w.z);
+  }
+  return surface_point(org, J.tkind == 1 ? p.sp_uc : p.sp_dc, J.tbeg + i);
+}
+
+// Cursor over a job's entries, 32 sources at a time: entry e, sources
+// [c0, c0 + 32).  It keeps the entry node's centre relative to the target
+// node's centre in FP32 (dlt, exact) and the entry node's radius (a power of
+// two).
+struct EntryCursor {
+  int e, eend, c0, kind, node, count, base;
+  float3 dlt;
+  float rad;
+  __device__ __forceinline__ void open(const P2PMixedParams& a, const float4 orgf) {
+    const P2PParams& p = a.p;
+    for (; e < eend; ++e) {
+      const int ent = p.entries[e];
+      kind = ent >> 28;
+      node = ent & 0x0fffffff;
+      count = kind == 0 ? p.src_num[node] : p.P;
+      base = kind == 0 ? p.src_beg[node] : 0;
+      if (count > 0) break;
+    }
+    if (e < eend) {
+      const float4 k = a.ctrf[node];
+      dlt = make_float3(k.x - orgf.x, k.y - orgf.y, k.z - orgf.z);
+      rad = k.w;
+    }
+  }
+  __device__ __forceinline__ void advance(const P2PMixedParams& a, const float4 orgf) {
+    c0 += 32;
+    if (c0 >= count) {
+      ++e;
+      c0 = 0;
+      open(a, orgf);
+    }
+  }
+  // Source c0 + lane of the current entry relative to the entry node's
+  // centre: the leaf point's stored offset, or rad * (FP32 unit-surface
+  // point), which is exact.  dlt is added when the chunk is written to the
+  // warp's buffer, so this load stays in flight across the pair loop.
+  __device__ __forceinline__ float4 source(const P2PMixedParams& a, int lane) const {
+    const int idx = c0 + lane;
+    if (kind == 0) return a.src4f[base + idx];
+    const float* sp = (kind == 1 ? a.spf_ue : a.spf_de) + 3 * idx;
+    const double w = (kind == 1 ? a.p.uden : a.p.dden)[(size_t)node * a.p.P + idx];
+    return make_float4(rad * sp[0], rad * sp[1], rad * sp[2], (float)w);
+  }
+};
+// Mixed form of a row job (see warp-autonomous P2P above): slot k of lane l
+// is target l + 32k; each chunk of 32 sources goes through the warp's shared
+// buffer in the target node's FP32 frame and is read back as broadcasts.
+template <int NS>
+__device__ __forceinline__ void warp_job_mixed(const P2PMixedParams& a, const P2PJob& J, int lane,
+                                               void* wbuf) {
+  const P2PParams& p = a.p;
+  const double4 org = p.ctr[J.tnode];
+  const float4 orgf = a.ctrf[J.tnode];
+  constexpr int NP2C = (NS + 1) / 2;
+  unsigned long long tx[NP2C], ty[NP2C], tz[NP2C];
+  {
+    float q[NS][3];
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+      const int i = lane + 32 * t;
+      double3 v = make_double3(org.x, org.y, org.z);
+      if (i < J.tcnt) v = job_target(p, J, org, i);
+      q[t][0] = (float)(v.x - org.x);
+      q[t][1] = (float)(v.y - org.y);
+      q[t][2] = (float)(v.z - org.z);
+    }
+#pragma unroll
+    for (int t = 0; t < NP2C; ++t) {
+      const int u = 2 * t + 1 < NS ? 2 * t + 1 : 2 * t;
+      tx[t] = pack2(q[2 * t][0], q[u][0]);
+      ty[t] = pack2(q[2 * t][1], q[u][1]);
+      tz[t] = pack2(q[2 * t][2], q[u][2]);
+    }
+  }
+  EntryCursor c{J.ebeg, J.eend, 0, 0, 0, 0, 0, make_float3(0.f, 0.f, 0.f), 0.f};
+  c.open(a, orgf);
+  float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (c.e < c.eend && lane < min(32, c.count)) s = c.source(a, lane);
+  double acc[NS];
+#pragma unroll
+  for (int t = 0; t < NS; ++t) acc[t] = 0.0;
+  ulonglong2* buf = (ulonglong2*)wbuf;
+  while (c.e < c.eend) {
+    const int cnt = min(32, c.count - c.c0);
+    const bool guard = c.kind == 0 && J.tkind == 0 && c.node == J.tnode;
+    if (lane < cnt) {
+      const float x = s.x + c.dlt.x, y = s.y + c.dlt.y, z = s.z + c.dlt.z;
+      buf[2 * lane] = make_ulonglong2(pack2(x, x), pack2(y, y));
+      buf[2 * lane + 1] = make_ulonglong2(pack2(z, z), pack2(s.w, s.w));
+    }
+    __syncwarp();
+    c.advance(a, orgf);
+    if (c.e < c.eend && lane < min(32, c.count - c.c0)) s = c.source(a, lane);
+    if (guard) pairs_mixed<NS, true>(tx, ty, tz, acc, buf, cnt);
+    else pairs_mixed<NS, false>(tx, ty, tz, acc, buf, cnt);
+    __syncwarp();
+  }
+#pragma unroll
+  for (int t = 0; t < NS; ++t) {
+    const int i = lane + 32 * t;
+    if (i < J.tcnt) {
+      const double r = kOOFP * acc[t];
+      double* o = p.out + J.out + i;
+      if (J.mode) *o += r;
+      else *o = r;
+    }
+  }
+}
+
+// Plain FP64 form of a row job: the same walk, sources staged as double4.
+template <int NS>
+__device__ __forceinline__ void warp_job_fp64(const P2PParams& p, const P2PJob& J, int lane,
+                                              void* wbuf) {
   const double4 org = p.ctr[J.tnode];
   double q[NS][3];
 #pragma unroll
@@ -305,45 +446,7 @@ __device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, in
   if (e < J.eend && lane < min(32, count - c0)) load_entry_source(p, kind, node, base, c0 + lane, s, w);
 
   double sum[NS];
-  if constexpr (kMixed) {
-    constexpr int NP2C = (NS + 1) / 2;
-    unsigned long long tx[NP2C], ty[NP2C], tz[NP2C];
-#pragma unroll
-    for (int t = 0; t < NP2C; ++t) {
-      const int u = 2 * t + 1 < NS ? 2 * t + 1 : 2 * t;
-      tx[t] = pack2((float)(q[2 * t][0] - org.x), (float)(q[u][0] - org.x));
-      ty[t] = pack2((float)(q[2 * t][1] - org.y), (float)(q[u][1] - org.y));
-      tz[t] = pack2((float)(q[2 * t][2] - org.z), (float)(q[u][2] - org.z));
-    }
-    double acc[NS];
-#pragma unroll
-    for (int t = 0; t < NS; ++t) acc[t] = 0.0;
-    ulonglong2* buf = (ulonglong2*)wbuf;
-    while (e < J.eend) {
-      const int cnt = min(32, count - c0);
-      const bool guard = kind == 0 && J.tkind == 0 && node == J.tnode;
-      if (lane < cnt) {
-        const float fx = (float)(s.x - org.x), fy = (float)(s.y - org.y),
-                    fz = (float)(s.z - org.z), fw = (float)w;
-        buf[2 * lane] = make_ulonglong2(pack2(fx, fx), pack2(fy, fy));
-        buf[2 * lane + 1] = make_ulonglong2(pack2(fz, fz), pack2(fw, fw));
-      }
-      __syncwarp();
-      c0 += 32;
-      if (c0 >= count) {
-        ++e;
-        c0 = 0;
-        open_entry();
-      }
-      if (e < J.eend && lane < min(32, count - c0))
-        load_entry_source(p, kind, node, base, c0 + lane, s, w);
-      if (guard) pairs_mixed<NS, true>(tx, ty, tz, acc, buf, cnt);
-      else pairs_mixed<NS, false>(tx, ty, tz, acc, buf, cnt);
-      __syncwarp();
-    }
-#pragma unroll
-    for (int t = 0; t < NS; ++t) sum[t] = acc[t];
-  } else {
+  {
     double tx[NS], ty[NS], tz[NS], acc[NS];
 #pragma unroll
     for (int t = 0; t < NS; ++t) {
@@ -385,15 +488,23 @@ __device__ __forceinline__ void warp_job(const P2PParams& p, const P2PJob& J, in
   }
 }
 
+template <bool kMixed, int NS>
+__device__ __forceinline__ void warp_job(const P2PArgs<kMixed>& a, const P2PJob& J, int lane,
+                                         void* wbuf) {
+  if constexpr (kMixed) warp_job_mixed<NS>(a, J, lane, wbuf);
+  else warp_job_fp64<NS>(a, J, lane, wbuf);
+}
+
 template <bool kMixed>
-__device__ __forceinline__ void run_job(const P2PParams& p, const P2PJob& J, int lane, void* wb) {
+__device__ __forceinline__ void run_job(const P2PArgs<kMixed>& a, const P2PJob& J, int lane,
+                                        void* wb) {
   switch ((J.tcnt + 31) >> 5) {
-    case 1: warp_job<kMixed, 1>(p, J, lane, wb); break;
-    case 2: warp_job<kMixed, 2>(p, J, lane, wb); break;
-    case 3: warp_job<kMixed, 3>(p, J, lane, wb); break;
-    case 4: warp_job<kMixed, 4>(p, J, lane, wb); break;
-    case 5: warp_job<kMixed, 5>(p, J, lane, wb); break;
-    default: warp_job<kMixed, kMaxSlots>(p, J, lane, wb); break;
+    case 1: warp_job<kMixed, 1>(a, J, lane, wb); break;
+    case 2: warp_job<kMixed, 2>(a, J, lane, wb); break;
+    case 3: warp_job<kMixed, 3>(a, J, lane, wb); break;
+    case 4: warp_job<kMixed, 4>(a, J, lane, wb); break;
+    case 5: warp_job<kMixed, 5>(a, J, lane, wb); break;
+    default: warp_job<kMixed, kMaxSlots>(a, J, lane, wb); break;
   }
 }
 
@@ -407,7 +518,7 @@ __device__ __forceinline__ int next_job_of_warp(int* next_job, int lane) {
 // counter is zeroed on the stream before every launch.
 template <bool kMixed>
 __global__ void __launch_bounds__(32 * kWarpJobsPerBlock, kMixed ? KFMM_P2P_MIXED_MINB : 4)
-p2p_warp_kernel(P2PParams p, int njobs, int* next_job) {
+p2p_warp_kernel(P2PArgs<kMixed> a, int njobs, int* next_job) {
   __shared__ __align__(16) unsigned char smem[kWarpJobsPerBlock][32 * 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   void* wb = smem[wid];
@@ -416,14 +527,14 @@ p2p_warp_kernel(P2PParams p, int njobs, int* next_job) {
     if (lane == 0) j = atomicAdd(next_job, 1);
     j = __shfl_sync(0xffffffffu, j, 0);
     if (j >= njobs) return;
-    const P2PJob J = p.jobs[j];
+    const P2PJob J = base_of(a).jobs[j];
     switch ((J.tcnt + 31) >> 5) {
-      case 1: warp_job<kMixed, 1>(p, J, lane, wb); break;
-      case 2: warp_job<kMixed, 2>(p, J, lane, wb); break;
-      case 3: warp_job<kMixed, 3>(p, J, lane, wb); break;
-      case 4: warp_job<kMixed, 4>(p, J, lane, wb); break;
-      case 5: warp_job<kMixed, 5>(p, J, lane, wb); break;
-      default: warp_job<kMixed, kMaxSlots>(p, J, lane, wb); break;
+      case 1: warp_job<kMixed, 1>(a, J, lane, wb); break;
+      case 2: warp_job<kMixed, 2>(a, J, lane, wb); break;
+      case 3: warp_job<kMixed, 3>(a, J, lane, wb); break;
+      case 4: warp_job<kMixed, 4>(a, J, lane, wb); break;
+      case 5: warp_job<kMixed, 5>(a, J, lane, wb); break;
+      default: warp_job<kMixed, kMaxSlots>(a, J, lane, wb); break;
     }
   }
 }
@@ -433,7 +544,7 @@ p2p_warp_kernel(P2PParams p, int njobs, int* next_job) {
 // describes.
 template <bool kMixed>
 __global__ void __launch_bounds__(32 * kWarpJobsPerBlock, kMixed ? KFMM_P2P_MIXED_MINB : 4)
-p2p_fused_kernel(const P2PParams* params, const int2* jobs, int njobs, int* next_job) {
+p2p_fused_kernel(const P2PArgs<kMixed>* params, const int2* jobs, int njobs, int* next_job) {
   __shared__ __align__(16) unsigned char smem[kWarpJobsPerBlock][32 * 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   void* wb = smem[wid];
@@ -441,8 +552,8 @@ p2p_fused_kernel(const P2PParams* params, const int2* jobs, int njobs, int* next
     const int j = next_job_of_warp(next_job, lane);
     if (j >= njobs) return;
     const int2 pj = jobs[j];
-    const P2PParams& p = params[pj.x];
-    run_job<kMixed>(p, p.jobs[pj.y], lane, wb);
+    const P2PArgs<kMixed>& a = params[pj.x];
+    run_job<kMixed>(a, base_of(a).jobs[pj.y], lane, wb);
   }
 }
 
@@ -1254,6 +1365,22 @@ __global__ void gather_points_kernel(int n, const int* perm, const double* x, co
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int k = perm[i];
     out[i] = make_double4(x[k], y[k], z[k], w ? w[k] : 0.0);
+  }
+}
+
+// Sources of a mixed-form plan: the leaf-order FP64 array as above, and the
+// same points as FP32 offsets from the centre of their leaf (leaf[i]) with
+// the density in FP32.
+__global__ void gather_sources_mixed_kernel(int n, const int* perm, const int* leaf,
+                                            const double* x, const double* y, const double* z,
+                                            const double* w, const double4* ctr, double4* out,
+                                            float4* outf) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int k = perm[i];
+    const double4 v = make_double4(x[k], y[k], z[k], w[k]);
+    const double4 c = ctr[leaf[i]];
+    out[i] = v;
+    outf[i] = make_float4((float)(v.x - c.x), (float)(v.y - c.y), (float)(v.z - c.z), (float)v.w);
   }
 }
 

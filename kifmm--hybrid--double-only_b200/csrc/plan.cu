@@ -79,6 +79,11 @@ struct kfmm_plan {
   double *o_sx = nullptr, *o_sy = nullptr, *o_sz = nullptr, *o_w = nullptr;
   double *o_tx = nullptr, *o_ty = nullptr, *o_tz = nullptr;
   double4 *src4 = nullptr, *trg4 = nullptr;
+  // mixed form: FP32 leaf-local sources and the leaf of each source; FP32
+  // node centres (exact: dyadic, depth <= 20)
+  float4* src4f = nullptr;
+  int* d_src_leaf = nullptr;
+  float4* ctrf = nullptr;
   double *pot_leaf = nullptr, *pot_orig = nullptr;
   bool have_src = false, have_trg = false;
   // expansions
@@ -89,6 +94,7 @@ struct kfmm_plan {
   double *d_uc2ue = nullptr, *d_ue2uc = nullptr, *d_dc2de = nullptr, *d_de2dc_stack = nullptr;
   void* d_trans = nullptr;
   double *d_sp_ue = nullptr, *d_sp_uc = nullptr, *d_sp_de = nullptr, *d_sp_dc = nullptr;
+  float *d_spf_ue = nullptr, *d_spf_de = nullptr;
   double *d_cs = nullptr, *d_sn = nullptr;
   int *d_surf_idx = nullptr, *d_surf_ijk = nullptr;
   // work lists
@@ -233,6 +239,16 @@ P2PParams p2p_params(const kfmm_plan* p, const P2PJob* jobs, const int* ent, dou
   return q;
 }
 
+P2PMixedParams p2p_mixed_params(const kfmm_plan* p, const P2PParams& q) {
+  P2PMixedParams m;
+  m.p = q;
+  m.src4f = p->src4f;
+  m.ctrf = p->ctrf;
+  m.spf_ue = p->d_spf_ue;
+  m.spf_de = p->d_spf_de;
+  return m;
+}
+
 FFTParams fft_params(const kfmm_plan* p) {
   FFTParams f{};
   f.np = p->np;
@@ -359,6 +375,20 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     ctr[i] = make_double4(c[0], c[1], c[2], 1.0 / double(1 << d->depth[i]));
   }
   KF_TRY(upload(p, &p->ctr, ctr));
+  {
+    std::vector<float4> cf(nn);
+    for (int i = 0; i < nn; ++i)
+      cf[i] = make_float4((float)ctr[i].x, (float)ctr[i].y, (float)ctr[i].z, (float)ctr[i].w);
+    KF_TRY(upload(p, &p->ctrf, cf));
+  }
+  if (p->prec == KFMM_MIXED) {
+    std::vector<int> leaf_of(d->num_src, 0);
+    for (int i = 0; i < nn; ++i)
+      if (d->child[i] == -1)
+        for (int k = 0; k < d->src_num[i]; ++k) leaf_of[d->src_beg[i] + k] = i;
+    KF_TRY(upload(p, &p->d_src_leaf, leaf_of));
+    KF_TRY(dalloc(p, &p->src4f, d->num_src));
+  }
   KF_TRY(upload(p, &p->d_depth, std::vector<int>(d->depth, d->depth + nn)));
   KF_TRY(upload(p, &p->d_src_beg, std::vector<int>(d->src_beg, d->src_beg + nn)));
   KF_TRY(upload(p, &p->d_src_num, std::vector<int>(d->src_num, d->src_num + nn)));
@@ -412,6 +442,8 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_TRY(upload(p, &p->d_sp_uc, S.uc));
   KF_TRY(upload(p, &p->d_sp_de, S.de));
   KF_TRY(upload(p, &p->d_sp_dc, S.dc));
+  KF_TRY(upload(p, &p->d_spf_ue, std::vector<float>(S.ue.begin(), S.ue.end())));
+  KF_TRY(upload(p, &p->d_spf_de, std::vector<float>(S.de.begin(), S.de.end())));
   {
     const int n = 2 * np;
     std::vector<double> cs(n), sn(n);
@@ -845,7 +877,8 @@ kfmm_status launch_p2p(const kfmm_plan* p, int which, int njobs, const P2PParams
   int* counter = p->job_counter + which;
   KF_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), S(stream)));
   if (p->prec == KFMM_MIXED)
-    p2p_warp_kernel<true><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(q, njobs, counter);
+    p2p_warp_kernel<true><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(
+        p2p_mixed_params(p, q), njobs, counter);
   else
     p2p_warp_kernel<false><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(q, njobs, counter);
   KF_CHECK_LAUNCH(std::string("p2p kernel (") + what + ")");
@@ -917,8 +950,14 @@ kfmm_status kfmm_set_sources_device(kfmm_plan* p, const double* sx, const double
     set_error("kfmm_set_sources_device: null argument");
     return KFMM_ERR_INVALID;
   }
-  gather_points_kernel<<<592, 256, 0, S(stream)>>>(p->ns, p->d_src_perm, sx, sy, sz, den, p->src4);
-  KF_CHECK_LAUNCH("gather_points_kernel");
+  if (p->prec == KFMM_MIXED) {
+    gather_sources_mixed_kernel<<<592, 256, 0, S(stream)>>>(p->ns, p->d_src_perm, p->d_src_leaf,
+                                                            sx, sy, sz, den, p->ctr, p->src4,
+                                                            p->src4f);
+  } else {
+    gather_points_kernel<<<592, 256, 0, S(stream)>>>(p->ns, p->d_src_perm, sx, sy, sz, den, p->src4);
+  }
+  KF_CHECK_LAUNCH("source gather");
   p->have_src = true;
   return KFMM_OK;
 }
@@ -1204,7 +1243,7 @@ struct kfmm_batch {
   cudaGraphExec_t exec = nullptr;
   // fused near field of all plans: per-plan kernel arguments, (plan, job)
   // pairs in cost-class order, the job counter
-  P2PParams* d_params = nullptr;
+  void* d_params = nullptr;  // P2PMixedParams (mixed plans) or P2PParams
   int2* d_jobs = nullptr;
   int* d_counter = nullptr;
 };
@@ -1265,12 +1304,15 @@ kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
   }
   fused = fused && njobs > 0 && njobs < (size_t)INT32_MAX;
   if (fused) {
+    const bool mixed = plans[0]->prec == KFMM_MIXED;
     std::vector<P2PParams> params(nplans);
+    std::vector<P2PMixedParams> mparams(mixed ? nplans : 0);
     std::vector<std::pair<float, int2>> order;
     order.reserve(njobs);
     for (int i = 0; i < nplans; ++i) {
       kfmm_plan* p = plans[i];
       params[i] = p2p_params(p, p->nf_jobs, p->nf_ent, p->pot_leaf);
+      if (mixed) mparams[i] = p2p_mixed_params(p, params[i]);
       for (int j = 0; j < p->n_nf; ++j) order.push_back({p->nf_class[j], make_int2(i, j)});
     }
     std::stable_sort(order.begin(), order.end(),
@@ -1279,12 +1321,13 @@ kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
                      });
     std::vector<int2> jobs(njobs);
     for (size_t j = 0; j < njobs; ++j) jobs[j] = order[j].second;
-    if ((e = cudaMalloc(&b->d_params, sizeof(P2PParams) * nplans)) != cudaSuccess ||
+    const size_t pbytes = mixed ? sizeof(P2PMixedParams) * nplans : sizeof(P2PParams) * nplans;
+    const void* psrc = mixed ? (const void*)mparams.data() : (const void*)params.data();
+    if ((e = cudaMalloc(&b->d_params, pbytes)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_jobs, sizeof(int2) * njobs)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_counter, sizeof(int))) != cudaSuccess)
       return fail(e, "cudaMalloc");
-    if ((e = cudaMemcpy(b->d_params, params.data(), sizeof(P2PParams) * nplans,
-                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+    if ((e = cudaMemcpy(b->d_params, psrc, pbytes, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(b->d_jobs, jobs.data(), sizeof(int2) * njobs, cudaMemcpyHostToDevice)) !=
             cudaSuccess)
       return fail(e, "cudaMemcpy");
@@ -1319,10 +1362,10 @@ kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
                                 (int)((njobs + kWarpJobsPerBlock - 1) / kWarpJobsPerBlock));
     if (plans[0]->prec == KFMM_MIXED)
       p2p_fused_kernel<true><<<blocks, 32 * kWarpJobsPerBlock, 0, origin>>>(
-          b->d_params, b->d_jobs, (int)njobs, b->d_counter);
+          (const P2PMixedParams*)b->d_params, b->d_jobs, (int)njobs, b->d_counter);
     else
       p2p_fused_kernel<false><<<blocks, 32 * kWarpJobsPerBlock, 0, origin>>>(
-          b->d_params, b->d_jobs, (int)njobs, b->d_counter);
+          (const P2PParams*)b->d_params, b->d_jobs, (int)njobs, b->d_counter);
     if (cudaGetLastError() != cudaSuccess) {
       set_error("kfmm_batch_create: fused near-field launch failed");
       st = KFMM_ERR_CUDA;
