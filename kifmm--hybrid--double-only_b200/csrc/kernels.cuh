@@ -343,6 +343,7 @@ struct EntryCursor {
     return make_float4(rad * sp[0], rad * sp[1], rad * sp[2], (float)w);
   }
 };
+
 // Mixed form of a row job (see warp-autonomous P2P above): slot k of lane l
 // is target l + 32k; each chunk of 32 sources goes through the warp's shared
 // buffer in the target node's FP32 frame and is read back as broadcasts.
