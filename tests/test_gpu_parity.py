@@ -213,10 +213,45 @@ def test_mixed_precision_accuracy(K, oracle_mod, cuda_ok, case):
 
 
 @pytest.mark.gpu
+def test_mixed_precision_deep_cluster(K, oracle_mod, cuda_ok):
+    """A tight cluster inside a uniform background drives the leaves to depth
+    ~17, where the mixed form's FP32 source offsets (relative to each leaf's
+    centre, plus the exact offset between centres) matter most: its rel-L2
+    error against the exact direct sum, on targets inside and outside the
+    cluster, stays within 2x the plain path's."""
+    rng = np.random.default_rng(17)
+
+    def cloud():
+        bg = rng.uniform(-1.0, 1.0, (30000, 3))
+        cl = np.array([0.1, -0.2, 0.3]) + rng.normal(0.0, 2e-5, (20000, 3))
+        return np.concatenate([bg, cl])
+
+    s, t = cloud(), cloud()
+    pts = {"sx": s[:, 0].copy(), "sy": s[:, 1].copy(), "sz": s[:, 2].copy(),
+           "tx": t[:, 0].copy(), "ty": t[:, 1].copy(), "tz": t[:, 2].copy(),
+           "den": rng.uniform(0.0, 1.0, len(s))}
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], 32)
+    depth = int(tree.array("depth").max())
+    assert 14 <= depth <= 20, depth
+    plain = K.Plan(tree, 4, K.PLAIN_FP64).evaluate(pts)
+    mixed = K.Plan(tree, 4, K.MIXED).evaluate(pts)
+    ids = np.concatenate([rng.choice(30000, 200, replace=False),
+                          30000 + rng.choice(20000, 200, replace=False)])
+    d = oracle_mod.direct(pts["tx"][ids], pts["ty"][ids], pts["tz"][ids], pts["sx"], pts["sy"],
+                          pts["sz"], pts["den"])
+    e_plain = np.linalg.norm(plain[ids] - d) / np.linalg.norm(d)
+    e_mixed = np.linalg.norm(mixed[ids] - d) / np.linalg.norm(d)
+    print(f"deep cluster (depth {depth}): rel-L2 vs direct: plain {e_plain:.3e} "
+          f"mixed {e_mixed:.3e}")
+    assert np.all(np.isfinite(mixed))
+    assert e_mixed <= 2.0 * e_plain
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("case", [("uniform", 65536, 128, 6, 0), ("ellipsoidSurface", 60000, 40, 4, 0),
                                   ("ellipseUniformAngles", 20000, 32, 3, 0)], ids=_ids)
 def test_mixed_downward_check_vs_plain(K, cuda_ok, case):
-    """The mixed form's V list (FP32 spectra and products, plane sums in
+    """The mixed form's V list (FP32 spectra and products, half-window sums in
     FP64) and S2L (FP32 P2P) against the plain path, on the downward check
     potentials they produce: per node max|d| / max|plain| <= 2e-5 (FP32
     rounding of the spectra and terms, ~6e-8 each, summed over up to 189
