@@ -185,15 +185,32 @@ kfmm_status add_gemm(kfmm_plan* p, std::vector<GemmBatch>& out, const double* A,
   KF_TRY(upload(p, &g.coff, coff));
   if (alpha) KF_TRY(upload(p, &g.alpha, *alpha));
   // rows in near-equal chunks of <= kGemmRows (multiples of 8); split K when
-  // the launch would give fewer than two blocks per SM
+  // the launch would give fewer than two blocks per SM.  The split count
+  // minimises (waves of blocks) x (16-deep K slices per block) plus the
+  // split-K partial sums' traffic, 16 B per entry per split, counted at
+  // ~12.5 MB per slice-wave (the kernel's measured rate): one wave of half-K
+  // blocks beats two waves of third-K blocks.
   g.chunks = (M + kGemmRows - 1) / kGemmRows;
   g.mrows = ((M + g.chunks - 1) / g.chunks + 7) / 8 * 8;
   const int blocks = g.chunks * ((g.ncol + kGemmBN - 1) / kGemmBN);
   const int want = 2 * p->num_sms;
   g.nsplit = 1;
-  if (blocks < want) g.nsplit = std::max(1, std::min((want + blocks - 1) / blocks, K / 64));
-  g.ksplit = ((K + g.nsplit - 1) / g.nsplit + kGemmBK - 1) / kGemmBK * kGemmBK;
-  g.nsplit = (K + g.ksplit - 1) / g.ksplit;
+  g.ksplit = (K + kGemmBK - 1) / kGemmBK * kGemmBK;
+  if (blocks < want) {
+    double best = 1e300;
+    for (int s = 1; s <= std::max(1, K / 64); ++s) {
+      const int ks = ((K + s - 1) / s + kGemmBK - 1) / kGemmBK * kGemmBK;
+      const int ns = (K + ks - 1) / ks;
+      const double waves = std::ceil((double)blocks * ns / want);
+      const double traffic = ns > 1 ? ns * 16.0 * M * (double)g.ncol / 12.5e6 : 0.0;
+      const double cost = waves * (ks / kGemmBK) + traffic;
+      if (cost < best) {
+        best = cost;
+        g.nsplit = ns;
+        g.ksplit = ks;
+      }
+    }
+  }
   if (g.nsplit > 1)
     p->splitk_doubles = std::max(p->splitk_doubles, (size_t)g.nsplit * g.ncol * M);
   p->stats.gemm_flops += 2.0 * M * (double)K * g.ncol;
