@@ -65,6 +65,9 @@ struct P2PMixedParams {
   const float4* ctrf;
   const float* spf_ue;  // the unit UE / DE surfaces in FP32, 3 per point
   const float* spf_de;
+  // near field: target i of a job goes to out[out_perm[J.out + i]], the
+  // original order (no scatter pass afterwards); null: out[J.out + i]
+  const int* out_perm;
 };
 template <bool kMixed>
 using P2PArgs = typename std::conditional<kMixed, P2PMixedParams, P2PParams>::type;
@@ -402,7 +405,7 @@ __device__ __forceinline__ void warp_job_mixed(const P2PMixedParams& a, const P2
     const int i = lane + 32 * t;
     if (i < J.tcnt) {
       const double r = kOOFP * acc[t];
-      double* o = p.out + J.out + i;
+      double* o = p.out + (a.out_perm ? a.out_perm[J.out + i] : J.out + i);
       if (J.mode) *o += r;
       else *o = r;
     }
@@ -1385,6 +1388,13 @@ __global__ void gather_sources_mixed_kernel(int n, const int* perm, const int* l
     out[i] = v;
     outf[i] = make_float4((float)(v.x - c.x), (float)(v.y - c.y), (float)(v.z - c.z), (float)v.w);
   }
+}
+
+// Leaf-order view of original-order potentials (introspection).
+__global__ void gather_pot_kernel(int n, const int* perm, const double* pot_orig,
+                                  double* pot_leaf) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    pot_leaf[i] = pot_orig[perm[i]];
 }
 
 __global__ void scatter_pot_kernel(int n, const int* perm, const double* pot_leaf,

@@ -256,14 +256,23 @@ P2PParams p2p_params(const kfmm_plan* p, const P2PJob* jobs, const int* ent, dou
   return q;
 }
 
-P2PMixedParams p2p_mixed_params(const kfmm_plan* p, const P2PParams& q) {
+P2PMixedParams p2p_mixed_params(const kfmm_plan* p, const P2PParams& q,
+                                const int* out_perm = nullptr) {
   P2PMixedParams m;
   m.p = q;
   m.src4f = p->src4f;
   m.ctrf = p->ctrf;
   m.spf_ue = p->d_spf_ue;
   m.spf_de = p->d_spf_de;
+  m.out_perm = out_perm;
   return m;
+}
+
+// The near field's output: the mixed form writes the potentials in original
+// order directly (its kernel takes the target permutation), the plain form
+// in leaf order for the scatter pass.
+double* near_field_out(const kfmm_plan* p) {
+  return p->prec == KFMM_MIXED ? p->pot_orig : p->pot_leaf;
 }
 
 FFTParams fft_params(const kfmm_plan* p) {
@@ -895,7 +904,7 @@ kfmm_status launch_p2p(const kfmm_plan* p, int which, int njobs, const P2PParams
   KF_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), S(stream)));
   if (p->prec == KFMM_MIXED)
     p2p_warp_kernel<true><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(
-        p2p_mixed_params(p, q), njobs, counter);
+        p2p_mixed_params(p, q, which == 2 ? p->d_trg_perm : nullptr), njobs, counter);
   else
     p2p_warp_kernel<false><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(q, njobs, counter);
   KF_CHECK_LAUNCH(std::string("p2p kernel (") + what + ")");
@@ -1099,16 +1108,19 @@ kfmm_status kfmm_ulist_calc(kfmm_plan* p, void* stream) {
     return KFMM_ERR_STATE;
   }
   if (p->n_nf) {
-    KF_TRY(launch_p2p(p, 2, p->n_nf, p2p_params(p, p->nf_jobs, p->nf_ent, p->pot_leaf), stream,
-                      "near field"));
+    KF_TRY(launch_p2p(p, 2, p->n_nf, p2p_params(p, p->nf_jobs, p->nf_ent, near_field_out(p)),
+                      stream, "near field"));
   }
   return KFMM_OK;
 }
 
 kfmm_status kfmm_copy_trg_val(kfmm_plan* p, double* pot_host, void* stream) {
   if (!p) return KFMM_ERR_INVALID;
-  scatter_pot_kernel<<<592, 256, 0, S(stream)>>>(p->nt, p->d_trg_perm, p->pot_leaf, p->pot_orig);
-  KF_CHECK_LAUNCH("scatter_pot_kernel");
+  if (p->prec != KFMM_MIXED) {  // the mixed near field wrote pot_orig itself
+    scatter_pot_kernel<<<592, 256, 0, S(stream)>>>(p->nt, p->d_trg_perm, p->pot_leaf,
+                                                   p->pot_orig);
+    KF_CHECK_LAUNCH("scatter_pot_kernel");
+  }
   if (pot_host) {
     KF_CUDA(cudaMemcpyAsync(pot_host, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToHost,
                             S(stream)));
@@ -1243,6 +1255,11 @@ kfmm_status kfmm_read_array(kfmm_plan* p, int which, double* out, size_t count) 
     return KFMM_ERR_INVALID;
   }
   KF_CUDA(cudaDeviceSynchronize());
+  if (which == 3 && p->prec == KFMM_MIXED) {  // leaf-order view of pot_orig
+    gather_pot_kernel<<<592, 256>>>(p->nt, p->d_trg_perm, p->pot_orig, p->pot_leaf);
+    KF_CHECK_LAUNCH("gather_pot_kernel");
+    KF_CUDA(cudaDeviceSynchronize());
+  }
   KF_CUDA(cudaMemcpy(out, src, count * sizeof(double), cudaMemcpyDeviceToHost));
   return KFMM_OK;
 }
@@ -1328,8 +1345,8 @@ kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
     order.reserve(njobs);
     for (int i = 0; i < nplans; ++i) {
       kfmm_plan* p = plans[i];
-      params[i] = p2p_params(p, p->nf_jobs, p->nf_ent, p->pot_leaf);
-      if (mixed) mparams[i] = p2p_mixed_params(p, params[i]);
+      params[i] = p2p_params(p, p->nf_jobs, p->nf_ent, near_field_out(p));
+      if (mixed) mparams[i] = p2p_mixed_params(p, params[i], p->d_trg_perm);
       for (int j = 0; j < p->n_nf; ++j) order.push_back({p->nf_class[j], make_int2(i, j)});
     }
     std::stable_sort(order.begin(), order.end(),
