@@ -38,11 +38,12 @@ FLOPS_PER_PAIR = 11.0   # reference convention, fmm/driver.cc:60
 # launch at this workload, from one ncu capture per form on a B200 of this
 # pool; the algorithmic bytes (sources, targets, potentials and downward
 # densities once each, FP64) are 348 MB.  The mixed form reads its sources
-# as 16-byte FP32 records (67 MB, L2-resident); the plain form's 32-byte
-# sources (134 MB) exceed L2, and the cost-ordered job queue brings some
-# back from DRAM (the order buys more time than the traffic costs: the
-# kernel is not HBM-bound).
-NEAR_FIELD_DRAM_BYTES = {"mixed": 387.1e6, "fp64": 610.4e6}
+# as 16-byte FP32 records (67 MB, L2-resident) and stores each potential at
+# its original index (8-byte scattered writes: partial sectors read and
+# written back); the plain form's 32-byte sources (134 MB) exceed L2, and the
+# cost-ordered job queue brings some back from DRAM (the order buys more
+# time than the traffic costs: the kernel is not HBM-bound).
+NEAR_FIELD_DRAM_BYTES = {"mixed": 533.6e6, "fp64": 610.4e6}
 # batched workload: independent solves, point counts log-uniform in
 # [4096, 262144], half uniform cube / half ellipsoid surface, NP in {3, 4},
 # leaf sizes from the autotuner, all solves in one CUDA graph
