@@ -149,10 +149,12 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* plan, void* stream); /* FFT, Hadamard, IF
 kfmm_status kfmm_xlist_calc(kfmm_plan* plan, void* stream); /* S2L part of X */
 kfmm_status kfmm_down_calc(kfmm_plan* plan, void* stream);  /* L2L */
 /* U list + W list + direct part of X + L2T, fused: each target's potential is
- * accumulated once, in registers, and written once. */
+ * accumulated once, in registers, and written once (KFMM_MIXED plans: already
+ * at the target's original index). */
 kfmm_status kfmm_ulist_calc(kfmm_plan* plan, void* stream);
 /* copy_trg_val (fmm/cuda.cu:2543-2565): potentials to original order on the
- * device; pot_host (may be NULL) additionally receives them (synchronous). */
+ * device (plain plans: a scatter; mixed plans: already there); pot_host (may
+ * be NULL) additionally receives them (synchronous). */
 kfmm_status kfmm_copy_trg_val(kfmm_plan* plan, double* pot_host, void* stream);
 kfmm_status kfmm_get_potentials_device(kfmm_plan* plan, double* pot_dev, void* stream);
 
