@@ -447,7 +447,7 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": aggregate_mpts(n, world, e2e_ms), "unit": "Mpts/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 7 * 8 * n, "d2h_bytes_per_step": 8 * n},
-        "gpu_launches": int(st["launches"]) * args.steps,
+        "gpu_launches": int(plans["mixed"].stats()["launches"]) * args.steps,
         "clocks": clk,
         "tree": {"nodes": st["num_nodes"], "u_pairs": pairs, "v_pairs": st["v_pairs"],
                  "build_s_host": tree_host_s, "build_s_device": tree_device_s},

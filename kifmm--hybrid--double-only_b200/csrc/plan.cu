@@ -858,7 +858,8 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
                       (p->prec == KFMM_MIXED ? (p->n_pairs > 0) + (p->n_singles > 0)
                                              : (p->n_groups > 0)) +
                       (p->n_ifft > 0) + (p->n_s2l > 0) +
-                      (int)p->down_gemms.size() + (p->n_nf > 0) + 1;
+                      (int)p->down_gemms.size() + (p->n_nf > 0) +
+                      (p->prec == KFMM_MIXED ? 0 : 1);  // the plain form's scatter pass
   for (int i = 0; i < 7; ++i) KF_CUDA(cudaEventCreate(&p->ev[i]));
   KF_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
   KF_CUDA(cudaEventCreateWithFlags(&p->side_done, cudaEventDisableTiming));
