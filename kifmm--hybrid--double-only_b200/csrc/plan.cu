@@ -1211,7 +1211,13 @@ kfmm_status kfmm_evaluate(kfmm_plan* p, const double* sx, const double* sy, cons
   KF_TRY(kfmm_copy_trg_val(p, nullptr, stream));
   mark(p, 6, st);
   KF_CUDA(cudaMemcpyAsync(pot, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToHost, st));
+  int err = 0;
+  KF_CUDA(cudaMemcpyAsync(&err, p->d_error, sizeof(int), cudaMemcpyDeviceToHost, st));
   KF_CUDA(cudaStreamSynchronize(st));
+  if (err) {
+    set_error("a kernel's bounded wait ran out (V-list translation tile copy)");
+    return KFMM_ERR_CUDA;
+  }
   return KFMM_OK;
 }
 
