@@ -148,6 +148,21 @@ def test_direct_evaluation_entry(K, oracle_mod, cuda_ok):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["plain", "mixed"])
+def test_leaf_order_potentials(K, cuda_ok, precision):
+    """kfmm_read_array(3) gives the potentials in leaf order, pot_leaf[i] =
+    pot[trg_perm[i]], in both forms (the mixed near field stores original
+    order itself; the leaf-order view is gathered on demand)."""
+    prec = K.PLAIN_FP64 if precision == "plain" else K.MIXED
+    pts = K.generate_points(12000, "ellipseUniformAngles", 0, 5)
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], 24)
+    plan = K.Plan(tree, 4, prec)
+    pot = plan.evaluate(pts)
+    leaf = plan.read(3, len(pot))
+    assert np.array_equal(leaf, pot[tree.array("trg_perm")])
+
+
+@pytest.mark.gpu
 def test_repeat_runs_identical(K, cuda_ok):
     """Same inputs, same plan: bitwise-identical results run to run."""
     pts = K.generate_points(15000, "ellipseUniformAngles", 0, 7)
