@@ -521,9 +521,13 @@ __device__ __forceinline__ int next_job_of_warp(int* next_job, int lane) {
 }
 
 // Persistent: each warp takes jobs from *next_job until none are left.  The
-// counter is zeroed on the stream before every launch.
-template <bool kMixed>
-__global__ void __launch_bounds__(32 * kWarpJobsPerBlock, kMixed ? KFMM_P2P_MIXED_MINB : 4)
+// counter is zeroed on the stream before every launch.  kMinBlocks: resident
+// blocks per SM asked of ptxas; the plan runs the mixed near field with 5
+// (96 registers, no spills) when W-list surfaces carry more than 1% of its
+// pairs: measured 8-11% faster on ellipsoid-surface clouds, 1-2% slower than
+// 6 on uniform ones, whatever the NP.
+template <bool kMixed, int kMinBlocks = kMixed ? KFMM_P2P_MIXED_MINB : 4>
+__global__ void __launch_bounds__(32 * kWarpJobsPerBlock, kMinBlocks)
 p2p_warp_kernel(P2PArgs<kMixed> a, int njobs, int* next_job) {
   __shared__ __align__(16) unsigned char smem[kWarpJobsPerBlock][32 * 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

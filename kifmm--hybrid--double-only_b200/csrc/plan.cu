@@ -106,6 +106,8 @@ struct kfmm_plan {
   int* d_error = nullptr;      // set by kernels whose bounded waits ran out
   int had32_groups_per_block = 0;
   int p2p_grid = 0;            // resident P2P blocks on the device
+  bool nf_minb5 = false;       // mixed near field with 5 resident blocks per SM
+  int p2p_grid5 = 0;
   std::vector<GemmBatch> up_gemms, down_gemms;
   int *fft_nodes = nullptr, *ifft_nodes = nullptr;
   int n_fft = 0, n_ifft = 0;
@@ -780,6 +782,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   {
     std::vector<P2PJob> jobs;
     std::vector<int> ent;
+    double w_pairs = 0.0;  // pairs with W-list UE surfaces
     for (int t = 0; t < nn; ++t) {
       if (!is_leaf(t) || !has_trg(t) || d->trg_num[t] == 0) continue;
       int e0 = (int)ent.size();
@@ -788,6 +791,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
         int s = d->w_idx[k];
         bool direct = is_leaf(s) && d->src_num[s] < P;  // fmm/omp.cc:675
         ent.push_back(direct ? s : ((1 << 28) | s));
+        if (!direct) w_pairs += (double)d->trg_num[t] * P;
       }
       if (d->trg_num[t] < P)  // fmm/omp.cc:724
         for (int k = d->x_ptr[t]; k < d->x_ptr[t + 1]; ++k) ent.push_back(d->x_idx[k]);
@@ -799,6 +803,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     }
     order_jobs(jobs, ent, &p->nf_class);
     p->n_nf = (int)jobs.size();
+    p->nf_minb5 = p->prec == KFMM_MIXED && w_pairs > 0.01 * p->stats.u_pairs;
     KF_TRY(upload(p, &p->nf_jobs, jobs));
     KF_TRY(upload(p, &p->nf_ent, ent));
   }
@@ -846,6 +851,12 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       KF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p2p_warp_kernel<false>,
                                                             32 * kWarpJobsPerBlock, 0));
     p->p2p_grid = std::max(1, occ) * p->num_sms;
+    if (p->nf_minb5) {
+      int occ5 = 0;
+      KF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, p2p_warp_kernel<true, 5>,
+                                                            32 * kWarpJobsPerBlock, 0));
+      p->p2p_grid5 = std::max(1, occ5) * p->num_sms;
+    }
   }
   p->stats.num_nodes = nn;
   p->stats.P = P;
@@ -903,7 +914,12 @@ kfmm_status launch_p2p(const kfmm_plan* p, int which, int njobs, const P2PParams
   const int blocks = std::min(p->p2p_grid, (njobs + kWarpJobsPerBlock - 1) / kWarpJobsPerBlock);
   int* counter = p->job_counter + which;
   KF_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), S(stream)));
-  if (p->prec == KFMM_MIXED)
+  if (p->prec == KFMM_MIXED && which == 2 && p->nf_minb5)
+    p2p_warp_kernel<true, 5><<<std::min(p->p2p_grid5, (njobs + kWarpJobsPerBlock - 1) /
+                                                          kWarpJobsPerBlock),
+                               32 * kWarpJobsPerBlock, 0, S(stream)>>>(
+        p2p_mixed_params(p, q, p->d_trg_perm), njobs, counter);
+  else if (p->prec == KFMM_MIXED)
     p2p_warp_kernel<true><<<blocks, 32 * kWarpJobsPerBlock, 0, S(stream)>>>(
         p2p_mixed_params(p, q, which == 2 ? p->d_trg_perm : nullptr), njobs, counter);
   else
