@@ -4,10 +4,14 @@ Workload (one "step" = one full FMM evaluation of a fixed synthetic problem):
 4,194,304 uniform points in [-1,1)^3 (the reference's "uniform" generator,
 srand48(26)), densities in [0,1), NP=6, at most 512 points per leaf.  Tree,
 lists and operators are built once (untimed, like the reference's preproc);
-`value` times kfmm_run with inputs resident in HBM; `e2e` times kfmm_evaluate
-from pinned host buffers (H2D of points and densities, the solve, D2H of the
-potentials).  Multi-GPU runs are replicas (one independent solve per rank,
-weak scaling, no collective on the data path).
+`value` times kfmm_run of the mixed form with inputs resident in HBM; `fp64`
+the plain form the same way; `e2e` times kfmm_evaluate from pinned host
+buffers (H2D of points and densities, the solve, D2H of the potentials).
+The CPU reference (`cpu_baseline`, and `--impl reference`) is the
+reference's own fmmd--omp_sse_block built from its sources, on the same
+4,194,304-point configuration, all host threads.  Multi-GPU runs are replicas
+(one independent solve per rank, weak scaling, no collective on the data
+path).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -32,23 +36,23 @@ PPB = 512
 DIST = "uniform"
 METRIC = "Mpts/s per FMM solve at 4M pts NP=6, mixed vs FP64 on B200, rel-L2 err vs FP64"
 WORKLOAD = "KIFMM Laplace solve, 4194304 uniform points, NP=6, 512 pts/box"
-CPU_SAMPLE_N = 1048576  # bounded sample for the CPU reference (same NP, leaf size, generator)
-FLOPS_PER_PAIR = 11.0   # reference convention, fmm/driver.cc:60
+FLOPS_PER_PAIR = 11.0    # reference convention, fmm/driver.cc:60
+FLOPS_PER_CMAC = 8.0     # complex multiply-add, fmm/driver.cc:82 (4 * 2F per V pair)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one near-field
-# launch at this workload, from one ncu capture per form on a B200 of this
-# pool; the algorithmic bytes (sources, targets, potentials and downward
-# densities once each, FP64) are 348 MB.  The mixed form reads its sources
-# as 16-byte FP32 records (67 MB, L2-resident) and stores each potential at
-# its original index (8-byte scattered writes: partial sectors read and
-# written back); the plain form's 32-byte sources (134 MB) exceed L2, and the
-# cost-ordered job queue brings some back from DRAM (the order buys more
-# time than the traffic costs: the kernel is not HBM-bound).
+# launch at this workload, from the latest ncu capture of each form on a B200
+# of this pool (profiles/p2p_near_field_4m_np6.md); the algorithmic bytes
+# (sources, targets, potentials and downward densities once each, FP64) are
+# 348 MB.
 NEAR_FIELD_DRAM_BYTES = {"mixed": 533.6e6, "fp64": 610.4e6}
 # batched workload: independent solves, point counts log-uniform in
 # [4096, 262144], half uniform cube / half ellipsoid surface, NP in {3, 4},
 # leaf sizes from the autotuner, all solves in one CUDA graph
 BATCH_SOLVES = 256
 BATCH_LEAF_CANDIDATES = (32, 64, 128, 256)
+# wall-clock budgets of the CPU reference runs (seconds): the timed steps of
+# `--impl reference`, and the cpu_baseline leg of the GPU arm
+REF_ARM_BUDGET_S = 200.0
+CPU_BASELINE_BUDGET_S = 45.0
 
 
 def parse():
@@ -92,6 +96,25 @@ def reduce_max(value, world, device):
 def aggregate_mpts(n_per_rank, world, ms):
     """Whole-job throughput: all ranks' points over the slowest rank's time."""
     return n_per_rank * world / (ms * 1e3)
+
+
+def sig(x, d=4):
+    """Round floats for the JSON line (it must fit a log tail)."""
+    if isinstance(x, float):
+        return float(f"{x:.{d}g}")
+    if isinstance(x, dict):
+        return {k: sig(v, d) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [sig(v, d) for v in x]
+    return x
+
+
+def config_of(n):
+    """The workload description shared by both arms (the reference arm runs
+    the same points, NP and leaf size)."""
+    return {"workload": WORKLOAD, "n_points": n, "np": NP, "pts_per_box": PPB,
+            "distribution": DIST, "parallelism": "single",
+            "l2": "inputs larger than L2 (points 268 MB; expansions and spectra >1 GB)"}
 
 
 class ClockSampler:
@@ -155,10 +178,23 @@ def measured_peaks():
         return {}
 
 
-def run_reference_cpu(n, steps, warmup):
+def _run_ref_once(exe, n, env):
+    t0 = time.time()
+    r = subprocess.run([exe, str(n), DIST, str(PPB)], env=env, capture_output=True, text=True,
+                       timeout=900)
+    m = re.search(r"Total Execution Time:\s*([0-9.eE+-]+)", r.stderr)
+    if r.returncode != 0 or not m:
+        raise RuntimeError("fmmd--omp_sse_block failed: " + r.stderr[-300:])
+    return float(m.group(1)), time.time() - t0
+
+
+def run_reference_cpu(n, max_steps, warmup, budget_s):
     """The reference's own blocked-SSE CPU evaluator (fmmd--omp_sse_block,
-    built from its sources into oracle/_ref), all host threads, on a bounded
-    sample of the workload.  Returns (Mpts/s median, per-run seconds, kind)."""
+    built from its sources into oracle/_ref) on the workload itself, all host
+    threads pinned.  `warmup` untimed runs, then up to `max_steps` timed runs
+    while the wall clock stays within `budget_s` (at least one).  Each run is
+    one process: input generation and tree build are outside the reference's
+    own 'Total Execution Time', which is what is timed."""
     import oracle  # noqa: F401  (checker package; only its build lives here)
     exe = os.path.join(ROOT, "oracle", "_ref", "fmmd--omp_sse_block")
     if not os.path.exists(exe):
@@ -168,62 +204,62 @@ def run_reference_cpu(n, steps, warmup):
     # pinned one per core
     env = dict(os.environ, NP=str(NP), NV="1", OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="true",
                OMP_PLACES="cores", GLIBC_TUNABLES="glibc.malloc.mmap_threshold=4096")
-    times = []
-    for i in range(warmup + steps):
-        r = subprocess.run([exe, str(n), DIST, str(PPB)], env=env, capture_output=True,
-                           text=True, timeout=900)
-        m = re.search(r"Total Execution Time:\s*([0-9.eE+-]+)", r.stderr)
-        if r.returncode != 0 or not m:
-            raise RuntimeError("fmmd--omp_sse_block failed: " + r.stderr[-300:])
-        if i >= warmup:
-            times.append(float(m.group(1)))
+    for _ in range(warmup):
+        _run_ref_once(exe, n, env)
+    times, t_start = [], time.time()
+    while len(times) < max(1, max_steps):
+        t, wall = _run_ref_once(exe, n, env)
+        times.append(t)
+        if time.time() - t_start + wall > budget_s:
+            break
     t = statistics.median(times)
     # The reference computes its operators (SVD pseudo-inverses, translation
     # spectra) inside its timed Up/Down phases; this library does so at plan
     # creation, outside the timed solve.  A run of 32,768 points (same NP and
-    # leaf size: every operator is built, the evaluation is ~3% of the
-    # sample's) estimates that precompute, which is then taken off, so the
-    # comparison times evaluation against evaluation.
+    # leaf size: every operator is built, the evaluation is a small share)
+    # estimates that precompute, which is then taken off, so the comparison
+    # times evaluation against evaluation.
     small = 32768
-    r = subprocess.run([exe, str(small), DIST, str(PPB)], env=env, capture_output=True,
-                       text=True, timeout=900)
-    m = re.search(r"Total Execution Time:\s*([0-9.eE+-]+)", r.stderr)
-    pre = float(m.group(1)) if r.returncode == 0 and m else 0.0
-    pre = min(pre, 0.9 * t)
+    pre, _ = _run_ref_once(exe, small, env)
+    pre = min(pre, 0.5 * t)
     return {"value": n / (t - pre) / 1e6, "unit": "Mpts/s", "cores": cores, "kind": "reference",
-            "seconds": times, "precompute_s": pre, "value_with_precompute": n / t / 1e6,
-            "sample": f"fmmd--omp_sse_block {n} {DIST} {PPB}, NP={NP}, OMP_NUM_THREADS={cores} "
-                      "(pinned); "
-                      "the reference's own 'Total Execution Time' minus its in-phase operator "
-                      f"precompute (estimated by a {small}-point run)"}
+            "runs": len(times), "seconds": times, "precompute_s": pre,
+            "value_with_precompute": n / t / 1e6,
+            "sample": f"fmmd--omp_sse_block {n} {DIST} {PPB} (the full workload), NP={NP}, "
+                      f"OMP_NUM_THREADS={cores} pinned; median 'Total Execution Time' of "
+                      f"{len(times)} runs minus the in-phase operator precompute (a {small}-point "
+                      "run)"}
 
 
 def reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    steps, warmup = max(1, min(args.steps, 5)), max(0, min(args.warmup, 1))
-    res = run_reference_cpu(CPU_SAMPLE_N, steps, warmup)
+    warmup = min(args.warmup, 1)
+    res = run_reference_cpu(N_POINTS, args.steps, warmup, REF_ARM_BUDGET_S)
     if res is None:
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref/fmmd--omp_sse_block not built"}))
         return
     v = res["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpts/s",
-            "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
+            "n_gpus": args.gpus, "steps": res["runs"], "warmup": warmup,
             "ms_per_step": 1e3 * statistics.median(res["seconds"]), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample_points": CPU_SAMPLE_N, "np": NP,
-                       "pts_per_box": PPB, "distribution": DIST},
+            "config": config_of(N_POINTS),
+            "steps_note": f"{res['runs']} of the {args.steps} requested steps fit the "
+                          f"{REF_ARM_BUDGET_S:.0f} s budget of this arm; warm-up capped at 1 "
+                          "(one CPU process per solve)",
             "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample",
                                                  "precompute_s", "value_with_precompute")},
             "e2e": {"value": v, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    print(json.dumps(sig(line)))
 
 
 def time_plan(K, plan, sh, stream, steps, warmup, barrier, world, dev):
-    """Device time per kfmm_run (max over ranks), phase breakdown, and the
-    near-field kernel alone (the dominant launch) on its own stream."""
+    """Device time per kfmm_run (max over ranks), phase and kernel-group
+    breakdown of one run, and the near-field kernel alone (the dominant
+    launch) on its launch stream."""
     import torch
     for _ in range(warmup):
         plan.run(sh)
@@ -239,9 +275,15 @@ def time_plan(K, plan, sh, stream, steps, warmup, barrier, world, dev):
     barrier()
     ms = reduce_max(e0.elapsed_time(e1) / steps, world, dev)
     plan.enable_timing(True)
-    plan.run(sh)
-    phases = plan.phase_times()
+    kt = {k: [] for k in K.Plan.KERNEL_PHASES}
+    ph = {}
+    for _ in range(3):
+        plan.run(sh)
+        for k, v in plan.kernel_times().items():
+            kt[k].append(v)
+        ph = plan.phase_times()
     plan.enable_timing(False)
+    kernels = {k: statistics.median(v) for k, v in kt.items()}
     nf_ms = []
     for _ in range(3):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -250,21 +292,18 @@ def time_plan(K, plan, sh, stream, steps, warmup, barrier, world, dev):
         b.record(stream)
         torch.cuda.synchronize()
         nf_ms.append(a.elapsed_time(b))
-    return ms, phases, statistics.median(nf_ms)
+    return ms, ph, kernels, statistics.median(nf_ms)
 
 
-def time_batched(K, count, stream, steps, warmup, dev):
+def time_batched(K, count, stream, steps, warmup):
     """The batched workload in both forms: device time of one graph launch
-    (all solves), solves/s and Mpts/s, and per-solve error of the mixed form
-    against the plain one on a subset."""
+    (all solves), Mpts/s, and per-solve distance of the mixed form to the
+    plain one."""
     import torch
     from kifmm_b200 import autotune, batched
     autotune.CANDIDATES = BATCH_LEAF_CANDIDATES
     sp = batched.specs(count)
-    out = {"solves": count, "total_points": sum(s["n"] for s in sp),
-           "workload": "independent solves, N log-uniform in [4096, 262144], half uniform cube / "
-                       "half ellipsoid surface, NP in {3,4}, leaf size from the autotuner, one "
-                       "CUDA graph launch", "leaf_candidates": list(BATCH_LEAF_CANDIDATES)}
+    out = {"solves": count, "points": sum(s["n"] for s in sp)}
     sh = stream.cuda_stream
     pots = {}
     for name, prec in (("mixed", K.MIXED), ("fp64", K.PLAIN_FP64)):
@@ -280,17 +319,62 @@ def time_batched(K, count, stream, steps, warmup, dev):
         b.record(stream)
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / steps
-        pots[name] = B.potentials()
-        out[name] = {"ms_per_batch": ms, "solves_per_s": count / (ms * 1e-3),
-                     "Mpts_per_s": B.total_points / (ms * 1e-3) / 1e6,
-                     "leaf_sizes": {k: v["ppb"] for k, v in table.picks.items()}}
+        pots[name] = B.potentials(sh)
+        out[name] = {"ms": ms, "Mpts_s": B.total_points / (ms * 1e-3) / 1e6}
         B.close()
     rel = [float(np.linalg.norm(m - p) / np.linalg.norm(p)) for m, p in zip(pots["mixed"],
                                                                             pots["fp64"])]
-    out["mixed_over_fp64"] = out["fp64"]["ms_per_batch"] / out["mixed"]["ms_per_batch"]
+    out["mixed_over_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
     out["rel_l2_mixed_vs_fp64_max"] = max(rel)
-    out["rel_l2_mixed_vs_fp64_median"] = float(np.median(rel))
     return out
+
+
+def phase_rooflines(K, st, kern_mixed, pipes, hbm_gbs):
+    """Per-kernel-group rooflines of one mixed solve: achieved rate, the
+    bound's peak and the fraction, plus the whole solve's roofline time (sum
+    of the per-group bound times) against the measured solve time."""
+    P, F = st["P"], st["F"]
+    fpad = (F + 31) // 32 * 32
+    nspec = st["spectra_bytes"] / (16.0 * F)  # boxes with a source or a target spectrum
+    mufu = pipes["fp32_rsqrt_tops"] * 1e12
+    fma32 = pipes["fp32_fma_tflops"] * 1e12
+    dmma = pipes["fp64_dmma_tflops"] * 1e12
+    hbm = hbm_gbs * 1e9
+    ms = kern_mixed
+    out = {}
+    bound_s = 0.0
+
+    def put(name, t_ms, achieved, peak, unit, bound_t):
+        nonlocal bound_s
+        out[name] = {"ms": t_ms, "achieved": achieved, "peak": peak, "unit": unit,
+                     "frac": achieved / peak if peak else None}
+        bound_s += bound_t
+
+    nf = st["u_pairs"] / (ms["near_field"] * 1e-3)
+    put("near_field", ms["near_field"], nf / 1e12, mufu / 1e12, "Tpairs/s (MUFU rsqrt)",
+        st["u_pairs"] / mufu)
+    s2m = st["s2m_pairs"] / max(ms["s2m"] * 1e-3, 1e-9)
+    put("s2m", ms["s2m"], s2m / 1e12, mufu / 1e12, "Tpairs/s (MUFU rsqrt)", st["s2m_pairs"] / mufu)
+    gemm_s = (ms["up_gemm"] + ms["down_gemm"]) * 1e-3
+    put("level_gemms", ms["up_gemm"] + ms["down_gemm"], st["gemm_flops"] / gemm_s / 1e12,
+        dmma / 1e12, "TFLOP/s (FP64 DMMA)", st["gemm_flops"] / dmma)
+    # V list against HBM: each kernel's compulsory bytes (spectra as complex
+    # FP32, one pass; the FFTs also read or write the P-value surfaces)
+    half = nspec / 2.0
+    b_fft = half * fpad * 8.0 + st["num_nodes"] * P * 8.0
+    b_had = 2.0 * half * fpad * 8.0
+    for name, b in (("fft_src", b_fft), ("ifft_trg", b_fft)):
+        put(name, ms[name], b / (ms[name] * 1e-3) / 1e9, hbm_gbs, "GB/s (HBM)", b / hbm)
+    had_flops = st["hadamard_cmacs"] * FLOPS_PER_CMAC
+    out["hadamard"] = {"ms": ms["hadamard"],
+                       "achieved": b_had / (ms["hadamard"] * 1e-3) / 1e9, "peak": hbm_gbs,
+                       "unit": "GB/s (HBM)", "frac": b_had / (ms["hadamard"] * 1e-3) / hbm,
+                       "fma_frac": had_flops / (ms["hadamard"] * 1e-3) / fma32}
+    bound_s += max(b_had / hbm, had_flops / fma32)
+    total_ms = sum(ms.values())
+    out["solve"] = {"roofline_ms": bound_s * 1e3, "measured_ms": total_ms,
+                    "frac": bound_s * 1e3 / total_ms}
+    return sig(out, 3)
 
 
 def main():
@@ -376,74 +460,64 @@ def main():
     cargs = [ctypes.cast(hp[k].data_ptr(), fp) for k in ("sx", "sy", "sz", "den", "tx", "ty",
                                                           "tz")] + [ctypes.cast(hout.data_ptr(), fp)]
     plan = plans["mixed"]
-    K.check(K.lib().kfmm_evaluate(plan.handle, *cargs, sh), "evaluate")
-    e2e_steps = max(1, min(args.steps, 5))
+    for _ in range(max(1, args.warmup)):
+        K.check(K.lib().kfmm_evaluate(plan.handle, *cargs, sh), "evaluate")
     barrier()
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    for _ in range(e2e_steps):
+    for _ in range(args.steps):
         K.check(K.lib().kfmm_evaluate(plan.handle, *cargs, sh), "evaluate")
     b.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = reduce_max(a.elapsed_time(b) / e2e_steps, world, dev)
+    e2e_ms = reduce_max(a.elapsed_time(b) / args.steps, world, dev)
     assert np.array_equal(hout.numpy(), pots["mixed"]), "e2e potentials differ from the resident run"
 
     peaks = measured_peaks()
+    hbm_gbs = peaks.get("hbm_gbs") or 6650.0
     pipes = K.measure_peaks()
     pairs = st["u_pairs"]
 
     def roof(name, nf_ms):
         rate = pairs / (nf_ms * 1e-3)
-        if name == "mixed":
-            ceil = pipes["fp32_rsqrt_tops"] * 1e12
-            bound, kern = "fp32 rsqrt (MUFU)", "p2p_warp_kernel<mixed> (near field: U+W+X+L2T)"
-        else:
-            ceil = pipes["fp64_rsqrt_tops"] * 1e12
-            bound, kern = "fp64 rsqrt", "p2p_warp_kernel<fp64> (near field: U+W+X+L2T)"
-        return {"bound": bound, "kernel": kern,
+        ceil = pipes["fp32_rsqrt_tops" if name == "mixed" else "fp64_rsqrt_tops"] * 1e12
+        return {"bound": "fp32 rsqrt (MUFU)" if name == "mixed" else "fp64 rsqrt",
+                "kernel": f"p2p_warp_kernel<{name}> near field (U+W+X+L2T)",
                 "achieved": FLOPS_PER_PAIR * rate / 1e12, "peak": FLOPS_PER_PAIR * ceil / 1e12,
                 "unit": "TFLOP/s", "frac": rate / ceil,
                 "traffic": NEAR_FIELD_DRAM_BYTES[name] if n == N_POINTS else None,
                 "algorithmic_bytes": 32.0 * n + 32.0 * n + 8.0 * n + 8.0 * st["num_nodes"] * st["P"],
                 "algorithmic": f"{FLOPS_PER_PAIR:g} flops/pair (fmm/driver.cc:60) x {pairs:.4e} "
-                               "pairs per launch; peak = one pair per measured reciprocal-sqrt "
-                               "issue",
-                "peak_source": "kfmm_measure_peak micro-benchmark, this run",
-                "pairs_per_s": rate, "launch_ms": nf_ms}
+                               "pairs/launch; peak = 1 pair per measured rsqrt",
+                "launch_ms": nf_ms}
 
     batched_res = None
     if not args.no_batched and args.batch > 0:
         batched_res = time_batched(K, args.batch, stream, max(1, min(args.steps, 5)),
-                                   max(1, args.warmup), dev)
+                                   max(1, args.warmup))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            r = run_reference_cpu(CPU_SAMPLE_N, 1, 0)
+            r = run_reference_cpu(n, 3, 0, CPU_BASELINE_BUDGET_S)
             if r:
                 cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample",
-                                         "precompute_s", "value_with_precompute")}
+                                         "precompute_s", "value_with_precompute", "runs")}
         except Exception as ex:  # reported, not fatal
             cpu = {"value": None, "error": str(ex)[:200]}
 
-    ms_mixed, ph_mixed, nf_mixed = res["mixed"]
-    ms_fp64, ph_fp64, nf_fp64 = res["fp64"]
+    ms_mixed, ph_mixed, kern_mixed, nf_mixed = res["mixed"]
+    ms_fp64, ph_fp64, kern_fp64, nf_fp64 = res["fp64"]
+    rl = roof("mixed", nf_mixed)
+    rl["phases"] = phase_rooflines(K, st, kern_mixed, pipes, hbm_gbs)
+    rl["peak_source"] = "kfmm_measure_peak micro-benchmarks (this run); HBM from MEASURED_PEAKS.json"
     line = {
         "metric": METRIC, "value": aggregate_mpts(n, world, ms_mixed), "unit": "Mpts/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64 (mixed)", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_points": n, "np": NP, "pts_per_box": PPB,
-                   "distribution": DIST, "precision": "mixed",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (points 268 MB; expansions and spectra >1 GB)"},
-        "rel_l2_err": err["mixed"], "rel_l2_vs_fp64": mixed_vs_fp64,
-        "fp64": {"value": aggregate_mpts(n, world, ms_fp64), "unit": "Mpts/s", "ms_per_step": ms_fp64,
-                 "rel_l2_err": err["fp64"], "phases_ms": ph_fp64, "roofline": roof("fp64", nf_fp64)},
-        "mixed_over_fp64": ms_fp64 / ms_mixed,
-        "phases_ms": ph_mixed,
-        "roofline": roof("mixed", nf_mixed),
+        "config": dict(config_of(n), parallelism=f"replicas x{world}" if world > 1 else "single"),
+        "roofline": rl,
         "cpu_baseline": cpu,
         "e2e": {"value": aggregate_mpts(n, world, e2e_ms), "unit": "Mpts/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 7 * 8 * n, "d2h_bytes_per_step": 8 * n},
@@ -451,12 +525,16 @@ def main():
         "clocks": clk,
         "tree": {"nodes": st["num_nodes"], "u_pairs": pairs, "v_pairs": st["v_pairs"],
                  "build_s_host": tree_host_s, "build_s_device": tree_device_s},
-        "hbm_peak_gbs": peaks.get("hbm_gbs"),
-        "measured_pipes": pipes,
         "batched": batched_res,
+        "phases_ms": ph_mixed,
+        "fp64": {"value": aggregate_mpts(n, world, ms_fp64), "ms_per_step": ms_fp64,
+                 "rel_l2_err": err["fp64"], "near_field_frac": roof("fp64", nf_fp64)["frac"],
+                 "phases_ms": ph_fp64},
+        "rel_l2_err": err["mixed"], "rel_l2_vs_fp64": mixed_vs_fp64,
+        "mixed_over_fp64": ms_fp64 / ms_mixed,
     }
     if rank == 0:
-        print(json.dumps(line))
+        print(json.dumps(sig(line)))
     for pl in plans.values():
         pl.close()
     tree.close()

@@ -154,9 +154,22 @@ kfmm_status kfmm_down_calc(kfmm_plan* plan, void* stream);  /* L2L */
 kfmm_status kfmm_ulist_calc(kfmm_plan* plan, void* stream);
 /* copy_trg_val (fmm/cuda.cu:2543-2565): potentials to original order on the
  * device (plain plans: a scatter; mixed plans: already there); pot_host (may
- * be NULL) additionally receives them (synchronous). */
+ * be NULL) additionally receives them (synchronous).
+ * kfmm_get_potentials_device copies them to device memory and waits for
+ * `stream`.  Both report KFMM_ERR_CUDA when a kernel of the last solve gave up
+ * a bounded wait (the mixed V list's translation-tile copy); the flag is
+ * cleared at the start of every solve, so a later solve that completes is
+ * reported as KFMM_OK again.  (The reference exits on any CUDA error,
+ * fmm/cuda.cu:19-30.) */
 kfmm_status kfmm_copy_trg_val(kfmm_plan* plan, double* pot_host, void* stream);
 kfmm_status kfmm_get_potentials_device(kfmm_plan* plan, double* pot_dev, void* stream);
+
+/* Tries of the bounded waits in the plan's kernels (no reference
+ * counterpart).  tries >= 0 sets the limit, tries < 0 restores the default
+ * (2^24).  A limit of 0 makes the V-list tile-copy wait give up at once: the
+ * solve then reports KFMM_ERR_CUDA, which tests use to drive the error path
+ * without a fault (the copy still lands before the kernel exits). */
+kfmm_status kfmm_set_wait_limit(kfmm_plan* plan, long long tries);
 
 /* End-to-end: host inputs (original order) -> host potentials. */
 kfmm_status kfmm_evaluate(kfmm_plan* plan, const double* sx, const double* sy,
@@ -193,6 +206,11 @@ kfmm_status kfmm_plan_stats(const kfmm_plan* plan, kfmm_stats* stats);
  * [up, vlist, xlist, down, ulist, copy].  enable != 0 records CUDA events. */
 kfmm_status kfmm_enable_timing(kfmm_plan* plan, int enable);
 kfmm_status kfmm_phase_times(const kfmm_plan* plan, float* ms6);
+/* Finer split of the same run (ms): [S2M pair sums, upward level products
+ * (UC2UE, M2M; includes zeroing the downward check potentials), forward FFT,
+ * Hadamard, inverse FFT, S2L, downward level products (L2L), near field,
+ * copy]. */
+kfmm_status kfmm_kernel_times(const kfmm_plan* plan, float* ms9);
 
 /* Allocation-free S2M for a batch of leaves; it has no counterpart in the
  * reference.  For callers that may not allocate device memory at call time
@@ -208,10 +226,13 @@ kfmm_status kfmm_phase_times(const kfmm_plan* plan, float* ms6);
  *   uden     device output, nleaves x P upward equivalent densities
  * Limit: nleaves * Q <= 1,048,576 (3542 leaves at NP=6); larger batches are
  * rejected with KFMM_ERR_INVALID.  The first call on a device sets that
- * device up (symbol addresses, a small surface table, synchronous) and should
- * come before any stream capture.  All calls on a device share the scratch:
- * calls that overlap on the GPU race and must be serialised by the caller.
- * No cudaMalloc/cudaFree or allocating library call is made. */
+ * device up (symbol addresses, a small surface table, then a device
+ * synchronisation) and should come before any stream capture; the set-up is
+ * remembered for the life of the process, so the device must not be reset
+ * (cudaDeviceReset) between calls.  All calls on a device share the scratch,
+ * which keeps the last call's contents: calls that overlap on the GPU race
+ * and must be serialised by the caller.  No cudaMalloc/cudaFree or
+ * allocating library call is made. */
 kfmm_status kfmm_s2m_noalloc(int np, int nleaves, const double* src4, const int* leaf_beg,
                              const int* leaf_num, const double* leaf_ctr, const double* uc2ue,
                              double* uden, void* stream);
@@ -230,6 +251,9 @@ typedef struct kfmm_batch kfmm_batch;
 kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
                               kfmm_batch** out);
 kfmm_status kfmm_batch_launch(kfmm_batch* batch, void* stream);
+/* Waits for `stream` and reports KFMM_ERR_CUDA if any solve of the last
+ * launch gave up a bounded wait (see kfmm_set_wait_limit). */
+kfmm_status kfmm_batch_wait(kfmm_batch* batch, void* stream);
 kfmm_status kfmm_batch_destroy(kfmm_batch* batch);
 
 /* Cost-model network (no counterpart in the reference, which takes the leaf

@@ -91,10 +91,13 @@ def lib():
         "kfmm_plan_stats": [vp, ctypes.POINTER(Stats)],
         "kfmm_enable_timing": [vp, i],
         "kfmm_phase_times": [vp, ctypes.POINTER(ctypes.c_float)],
+        "kfmm_kernel_times": [vp, ctypes.POINTER(ctypes.c_float)],
         "kfmm_measure_peak": [i, _f64p],
         "kfmm_s2m_noalloc": [i, i, vp, vp, vp, vp, vp, vp, vp],
         "kfmm_batch_create": [ctypes.POINTER(vp), i, i, ctypes.POINTER(vp)],
         "kfmm_batch_launch": [vp, vp],
+        "kfmm_batch_wait": [vp, vp],
+        "kfmm_set_wait_limit": [vp, ctypes.c_longlong],
         "kfmm_batch_destroy": [vp],
         "kfmm_mlp_param_count": [i, i, i, ctypes.POINTER(ctypes.c_longlong)],
         "kfmm_mlp_forward": [i, i, i, _f32p, i, _f32p, _f32p],
@@ -269,6 +272,10 @@ class Plan:
         check(lib().kfmm_plan_stats(self.handle, ctypes.byref(s)), "plan_stats")
         return {f: getattr(s, f) for f, _ in Stats._fields_}
 
+    def set_wait_limit(self, tries):
+        """Tries of the kernels' bounded waits; < 0 restores the default."""
+        check(lib().kfmm_set_wait_limit(self.handle, tries), "set_wait_limit")
+
     def enable_timing(self, on=True):
         check(lib().kfmm_enable_timing(self.handle, 1 if on else 0), "enable_timing")
 
@@ -276,6 +283,15 @@ class Plan:
         ms = (ctypes.c_float * 6)()
         check(lib().kfmm_phase_times(self.handle, ms), "phase_times")
         return dict(zip(("up", "vlist", "xlist", "down", "ulist", "copy"), list(ms)))
+
+    KERNEL_PHASES = ("s2m", "up_gemm", "fft_src", "hadamard", "ifft_trg", "s2l", "down_gemm",
+                     "near_field", "copy")
+
+    def kernel_times(self):
+        """Per-kernel-group device times (ms) of the last timed run."""
+        ms = (ctypes.c_float * 9)()
+        check(lib().kfmm_kernel_times(self.handle, ms), "kernel_times")
+        return dict(zip(self.KERNEL_PHASES, list(ms)))
 
     def close(self):
         if self.handle:
@@ -304,6 +320,11 @@ class Batch:
 
     def launch(self, stream=None):
         check(lib().kfmm_batch_launch(self.handle, stream), "batch_launch")
+
+    def wait(self, stream=None):
+        """Wait for the last launch; raise if one of its solves gave up a
+        bounded wait."""
+        check(lib().kfmm_batch_wait(self.handle, stream), "batch_wait")
 
     def close(self):
         if self.handle:

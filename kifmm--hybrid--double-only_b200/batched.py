@@ -45,7 +45,8 @@ class BatchedSolves:
     def launch(self, stream=None):
         self.batch.launch(stream)
 
-    def potentials(self):
+    def potentials(self, stream=None):
+        self.batch.wait(stream)
         return [s["plan"].potentials() for s in self.solves]
 
     def close(self):

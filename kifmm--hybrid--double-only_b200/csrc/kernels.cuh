@@ -1117,6 +1117,7 @@ struct Had32Params {
   const float2* spec;
   float2* effv;
   int* error;  // set to 1 when the tile copy does not complete
+  long long wait_limit;  // tries of the tile-copy wait (kMbarSpinLimit by default)
 };
 
 __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
@@ -1130,18 +1131,21 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
   return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
-  for (long long i = 0; i < kMbarSpinLimit; ++i)
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity,
+                                                  long long limit = kMbarSpinLimit) {
+  for (long long i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
 
 // Bulk-copies the translation tile of frequency block fb into dst (one
-// thread issues, all wait on the mbarrier with a bounded spin).  Returns false
-// in every thread of the block, after setting *error, if the copy did not
-// complete.
+// thread issues, all wait on the mbarrier with a bounded spin of `limit`
+// tries).  Returns false in every thread of the block, after setting *error,
+// if the copy did not complete; thread 0 then waits (with the full default
+// bound) for the copy still in flight to land before the block exits.
 __device__ __forceinline__ bool had32_load_tile(const float2* tile, int fb, unsigned char* dst,
-                                                unsigned long long* bar, int* error) {
+                                                unsigned long long* bar, int* error,
+                                                long long limit) {
   const unsigned b = smem_addr(bar);
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
@@ -1163,7 +1167,7 @@ __device__ __forceinline__ bool had32_load_tile(const float2* tile, int fb, unsi
           "l"(src + (size_t)c * chunk), "r"(chunk), "r"(b)
           : "memory");
   }
-  const bool ready = mbar_wait_bounded(b, 0);
+  const bool ready = mbar_wait_bounded(b, 0, limit);
   if (!__syncthreads_and(ready)) {
     if (threadIdx.x == 0) {
       atomicExch(error, 1);
@@ -1185,7 +1189,7 @@ __global__ void __launch_bounds__(kHad32Threads, 1) hadamard_fp32_kernel(Had32Pa
   const int g0 = blockIdx.x * p.groups_per_block;
   const int g1 = min(p.ngroups, g0 + p.groups_per_block);
   const size_t fbase = (size_t)fb * p.nn;
-  if (!had32_load_tile(p.tile, fb, had32_dyn, &bar, p.error)) return;
+  if (!had32_load_tile(p.tile, fb, had32_dyn, &bar, p.error, p.wait_limit)) return;
   for (int g = g0 + slot; g < g1; g += kHad32Warps) {
     for (int q = f; q < 216; q += 32) win[slot][q] = p.win[(size_t)g * 216 + q];
     if (f < 8) mem[slot][f] = p.members[(size_t)g * 8 + f];
@@ -1278,6 +1282,7 @@ struct HadPairParams {
   const float2* spec;
   float2* effv;
   int* error;
+  long long wait_limit;
 };
 
 __global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(HadPairParams p) {
@@ -1292,7 +1297,7 @@ __global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(
   const int g0 = blockIdx.x * p.pairs_per_block;
   const int g1 = min(p.npairs, g0 + p.pairs_per_block);
   const size_t fbase = (size_t)fb * p.nn;
-  if (!had32_load_tile(p.tile, fb, had32_dyn, &bar, p.error)) return;
+  if (!had32_load_tile(p.tile, fb, had32_dyn, &bar, p.error, p.wait_limit)) return;
   for (int g = g0 + slot; g < g1; g += kHadPairWarps) {
     for (int q = f; q < 288; q += 32) win[slot][q] = p.win[(size_t)g * 288 + q];
     if (f < 16) mem[slot][f] = p.members[(size_t)g * 16 + f];

@@ -14,6 +14,11 @@
 // it keeps the last call's contents; every call overwrites the part it uses
 // before reading it.  Calls whose work overlaps on the GPU (e.g. issued on two
 // streams at once) race on it and must be serialised by the caller.
+//
+// The per-device set-up (symbol addresses, the surface table) is done once
+// and remembered for the life of the process; a cudaDeviceReset between calls
+// would discard the table behind that record, so callers must not reset a
+// device they keep using through this entry point.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -120,8 +125,12 @@ kfmm_status setup_device(int dev, DeviceSetup** out) {
       std::copy(S.uc.begin(), S.uc.end(), tab.begin() + (size_t)(np - 3) * 3 * kMaxQ);
     }
     e = cudaMemcpyToSymbol(g_uc_surface, tab.data(), sizeof(double) * tab.size());
+    // A copy from pageable memory may return before the data has landed;
+    // the kernels run on the caller's stream, which need not wait on the
+    // legacy stream, so the table is made complete here.
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
-      set_error(std::string("kfmm_s2m_noalloc: cudaMemcpyToSymbol: ") + cudaGetErrorString(e));
+      set_error(std::string("kfmm_s2m_noalloc: surface table upload: ") + cudaGetErrorString(e));
       return KFMM_ERR_CUDA;
     }
     s.done = true;

@@ -103,7 +103,8 @@ struct kfmm_plan {
   int n_s2m = 0, n_nf = 0, n_s2l = 0;
   std::vector<float> nf_class;  // cost class of each near-field job (-log1.25 cost)
   int* job_counter = nullptr;  // persistent P2P work counters: S2M, S2L, near field
-  int* d_error = nullptr;      // set by kernels whose bounded waits ran out
+  int* d_error = nullptr;      // set by kernels whose bounded waits ran out; zeroed per solve
+  long long wait_limit = kMbarSpinLimit;  // tries of the V-list tile-copy wait
   int had32_groups_per_block = 0;
   int p2p_grid = 0;            // resident P2P blocks on the device
   bool nf_minb5 = false;       // mixed near field with 5 resident blocks per SM
@@ -123,8 +124,11 @@ struct kfmm_plan {
   double* splitk = nullptr;   // split-K partial sums, shared by the level GEMMs
   size_t splitk_doubles = 0;
   bool timing = false;
-  cudaEvent_t ev[7] = {};
-  float phase_ms[6] = {};
+  // timing marks (kfmm_enable_timing): 0 start, 1 S2M pairs done, 2 up done,
+  // 3 forward FFT, 4 Hadamard, 5 inverse FFT (V done), 6 S2L (X done),
+  // 7 down done, 8 near field done, 9 copy done
+  static constexpr int kMarks = 10;
+  cudaEvent_t ev[kMarks] = {};
   // kfmm_evaluate uploads the targets on a second stream while the far field
   // (which needs only the sources) runs
   cudaStream_t side = nullptr;
@@ -871,7 +875,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
                       (p->n_ifft > 0) + (p->n_s2l > 0) +
                       (int)p->down_gemms.size() + (p->n_nf > 0) +
                       (p->prec == KFMM_MIXED ? 0 : 1);  // the plain form's scatter pass
-  for (int i = 0; i < 7; ++i) KF_CUDA(cudaEventCreate(&p->ev[i]));
+  for (int i = 0; i < kfmm_plan::kMarks; ++i) KF_CUDA(cudaEventCreate(&p->ev[i]));
   KF_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
   KF_CUDA(cudaEventCreateWithFlags(&p->side_done, cudaEventDisableTiming));
   KF_CUDA(cudaEventCreateWithFlags(&p->src_done, cudaEventDisableTiming));
@@ -932,6 +936,19 @@ void mark(kfmm_plan* p, int i, cudaStream_t st) {
   if (p->timing) cudaEventRecord(p->ev[i], st);
 }
 
+// Waits for `stream` and reports whether a kernel of the plan's last solve
+// gave up a bounded wait (the flag is zeroed at the start of every V list).
+kfmm_status sync_and_check(kfmm_plan* p, cudaStream_t st) {
+  int err = 0;
+  KF_CUDA(cudaMemcpyAsync(&err, p->d_error, sizeof(int), cudaMemcpyDeviceToHost, st));
+  KF_CUDA(cudaStreamSynchronize(st));
+  if (err) {
+    set_error("a kernel's bounded wait ran out (V-list translation tile copy)");
+    return KFMM_ERR_CUDA;
+  }
+  return KFMM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -978,7 +995,7 @@ kfmm_status kfmm_plan_create_with_operators(const kfmm_tree_desc* tree, int np,
 kfmm_status kfmm_plan_destroy(kfmm_plan* p) {
   if (!p) return KFMM_OK;
   for (void* v : p->allocs) cudaFree(v);
-  for (int i = 0; i < 7; ++i)
+  for (int i = 0; i < kfmm_plan::kMarks; ++i)
     if (p->ev[i]) cudaEventDestroy(p->ev[i]);
   if (p->side_done) cudaEventDestroy(p->side_done);
   if (p->src_done) cudaEventDestroy(p->src_done);
@@ -1053,12 +1070,16 @@ kfmm_status kfmm_up_calc(kfmm_plan* p, void* stream) {
     KF_TRY(launch_p2p(p, 0, p->n_s2m, p2p_params(p, p->s2m_jobs, p->s2m_ent, p->chk_up), stream,
                       "s2m"));
   }
+  mark(p, 1, S(stream));
   return launch_gemms(p, p->up_gemms, S(stream));
 }
 
 kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
   if (!p) return KFMM_ERR_INVALID;
+  // the error flag reports this solve's waits only
+  KF_CUDA(cudaMemsetAsync(p->d_error, 0, sizeof(int), S(stream)));
   KF_CUDA(cudaMemsetAsync(p->dchk, 0, sizeof(double) * (size_t)p->nn * p->P, S(stream)));
+  mark(p, 2, S(stream));
   FFTParams f = fft_params(p);
   const bool mixed = p->prec == KFMM_MIXED;
   if (p->n_fft) {
@@ -1067,13 +1088,14 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
     f.specout = p->spec;
     KF_TRY(launch_fft(p->np, mixed, true, p->n_fft, f, stream));
   }
+  mark(p, 3, S(stream));
   if (p->n_groups) {
     if (mixed) {
       if (p->n_pairs) {
         const int ppb = p->pair_per_block;
         HadPairParams h{p->nn, p->n_pairs, ppb, p->pair_win, p->pair_members,
                         (const float2*)p->d_trans, (const float2*)p->spec, (float2*)p->effv,
-                        p->d_error};
+                        p->d_error, p->wait_limit};
         dim3 grid((p->n_pairs + ppb - 1) / ppb, p->Fpad / kFB);
         hadamard_fp32_pair_kernel<<<grid, kHadPairThreads, kHadPairSmemBytes, S(stream)>>>(h);
         KF_CHECK_LAUNCH("hadamard_fp32_pair_kernel");
@@ -1082,7 +1104,7 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
         const int gpb = p->had32_groups_per_block;
         Had32Params h{p->nn, p->n_singles, gpb, p->single_win, p->single_members,
                       (const float2*)p->d_trans, (const float2*)p->spec, (float2*)p->effv,
-                      p->d_error};
+                      p->d_error, p->wait_limit};
         dim3 grid((p->n_singles + gpb - 1) / gpb, p->Fpad / kFB);
         hadamard_fp32_kernel<<<grid, kHad32Threads, kHad32TileBytes, S(stream)>>>(h);
         KF_CHECK_LAUNCH("hadamard_fp32_kernel");
@@ -1096,6 +1118,7 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
       KF_CHECK_LAUNCH("hadamard_kernel");
     }
   }
+  mark(p, 4, S(stream));
   if (p->n_ifft) {
     f.nodes = p->ifft_nodes;
     f.specin = p->effv;
@@ -1141,13 +1164,7 @@ kfmm_status kfmm_copy_trg_val(kfmm_plan* p, double* pot_host, void* stream) {
   if (pot_host) {
     KF_CUDA(cudaMemcpyAsync(pot_host, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToHost,
                             S(stream)));
-    int err = 0;
-    KF_CUDA(cudaMemcpyAsync(&err, p->d_error, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
-    KF_CUDA(cudaStreamSynchronize(S(stream)));
-    if (err) {
-      set_error("a kernel's bounded wait ran out (V-list translation tile copy)");
-      return KFMM_ERR_CUDA;
-    }
+    return sync_and_check(p, S(stream));
   }
   return KFMM_OK;
 }
@@ -1156,6 +1173,12 @@ kfmm_status kfmm_get_potentials_device(kfmm_plan* p, double* pot_dev, void* stre
   if (!p || !pot_dev) return KFMM_ERR_INVALID;
   KF_CUDA(cudaMemcpyAsync(pot_dev, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToDevice,
                           S(stream)));
+  return sync_and_check(p, S(stream));
+}
+
+kfmm_status kfmm_set_wait_limit(kfmm_plan* p, long long tries) {
+  if (!p) return KFMM_ERR_INVALID;
+  p->wait_limit = tries < 0 ? kMbarSpinLimit : tries;
   return KFMM_OK;
 }
 
@@ -1167,13 +1190,12 @@ kfmm_status run_far_field(kfmm_plan* p, void* stream) {
   cudaStream_t st = S(stream);
   mark(p, 0, st);
   KF_TRY(kfmm_up_calc(p, stream));
-  mark(p, 1, st);
   KF_TRY(kfmm_vlist_calc(p, stream));
-  mark(p, 2, st);
+  mark(p, 5, st);
   KF_TRY(kfmm_xlist_calc(p, stream));
-  mark(p, 3, st);
+  mark(p, 6, st);
   KF_TRY(kfmm_down_calc(p, stream));
-  mark(p, 4, st);
+  mark(p, 7, st);
   return KFMM_OK;
 }
 }  // namespace
@@ -1191,9 +1213,9 @@ kfmm_status kfmm_run(kfmm_plan* p, void* stream) {
   }
   KF_TRY(run_far_field(p, stream));
   KF_TRY(kfmm_ulist_calc(p, stream));
-  mark(p, 5, S(stream));
+  mark(p, 8, S(stream));
   KF_TRY(kfmm_copy_trg_val(p, nullptr, stream));
-  mark(p, 6, S(stream));
+  mark(p, 9, S(stream));
   return KFMM_OK;
 }
 
@@ -1223,18 +1245,11 @@ kfmm_status kfmm_evaluate(kfmm_plan* p, const double* sx, const double* sy, cons
   KF_CUDA(cudaEventRecord(p->side_done, p->side));
   KF_CUDA(cudaStreamWaitEvent(st, p->side_done, 0));
   KF_TRY(kfmm_ulist_calc(p, stream));
-  mark(p, 5, st);
+  mark(p, 8, st);
   KF_TRY(kfmm_copy_trg_val(p, nullptr, stream));
-  mark(p, 6, st);
+  mark(p, 9, st);
   KF_CUDA(cudaMemcpyAsync(pot, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToHost, st));
-  int err = 0;
-  KF_CUDA(cudaMemcpyAsync(&err, p->d_error, sizeof(int), cudaMemcpyDeviceToHost, st));
-  KF_CUDA(cudaStreamSynchronize(st));
-  if (err) {
-    set_error("a kernel's bounded wait ran out (V-list translation tile copy)");
-    return KFMM_ERR_CUDA;
-  }
-  return KFMM_OK;
+  return sync_and_check(p, st);
 }
 
 kfmm_status kfmm_direct_evaluation(int nt, const double* tx, const double* ty, const double* tz,
@@ -1303,6 +1318,7 @@ struct kfmm_batch {
   void* d_params = nullptr;  // P2PMixedParams (mixed plans) or P2PParams
   int2* d_jobs = nullptr;
   int* d_counter = nullptr;
+  std::vector<kfmm_plan*> plans;  // for the error flags kfmm_batch_wait reads
 };
 
 static void batch_release(kfmm_batch* b) {
@@ -1331,6 +1347,7 @@ kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
     }
   nstreams = std::min(nstreams, nplans);
   kfmm_batch* b = new kfmm_batch();
+  b->plans.assign(plans, plans + nplans);
   auto fail = [&](cudaError_t e, const char* what) {
     set_error(std::string("kfmm_batch_create: ") + what + ": " + cudaGetErrorString(e));
     batch_release(b);
@@ -1453,6 +1470,25 @@ kfmm_status kfmm_batch_launch(kfmm_batch* b, void* stream) {
   return KFMM_OK;
 }
 
+kfmm_status kfmm_batch_wait(kfmm_batch* b, void* stream) {
+  if (!b) {
+    set_error("kfmm_batch_wait: null batch");
+    return KFMM_ERR_INVALID;
+  }
+  std::vector<int> err(b->plans.size(), 0);
+  for (size_t i = 0; i < b->plans.size(); ++i)
+    KF_CUDA(cudaMemcpyAsync(&err[i], b->plans[i]->d_error, sizeof(int), cudaMemcpyDeviceToHost,
+                            S(stream)));
+  KF_CUDA(cudaStreamSynchronize(S(stream)));
+  for (size_t i = 0; i < err.size(); ++i)
+    if (err[i]) {
+      set_error("kfmm_batch_wait: a bounded wait ran out in solve " + std::to_string(i) +
+                " (V-list translation tile copy)");
+      return KFMM_ERR_CUDA;
+    }
+  return KFMM_OK;
+}
+
 kfmm_status kfmm_batch_destroy(kfmm_batch* b) {
   batch_release(b);
   return KFMM_OK;
@@ -1470,8 +1506,21 @@ kfmm_status kfmm_phase_times(const kfmm_plan* p, float* ms) {
     set_error("kfmm_phase_times: timing not enabled");
     return KFMM_ERR_STATE;
   }
-  KF_CUDA(cudaEventSynchronize(p->ev[6]));
-  for (int i = 0; i < 6; ++i) KF_CUDA(cudaEventElapsedTime(&ms[i], p->ev[i], p->ev[i + 1]));
+  KF_CUDA(cudaEventSynchronize(p->ev[9]));
+  const int edge[7] = {0, 2, 5, 6, 7, 8, 9};  // up, vlist, xlist, down, ulist, copy
+  for (int i = 0; i < 6; ++i)
+    KF_CUDA(cudaEventElapsedTime(&ms[i], p->ev[edge[i]], p->ev[edge[i + 1]]));
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_kernel_times(const kfmm_plan* p, float* ms) {
+  if (!p || !ms) return KFMM_ERR_INVALID;
+  if (!p->timing) {
+    set_error("kfmm_kernel_times: timing not enabled");
+    return KFMM_ERR_STATE;
+  }
+  KF_CUDA(cudaEventSynchronize(p->ev[9]));
+  for (int i = 0; i < 9; ++i) KF_CUDA(cudaEventElapsedTime(&ms[i], p->ev[i], p->ev[i + 1]));
   return KFMM_OK;
 }
 

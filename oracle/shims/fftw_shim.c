@@ -9,6 +9,11 @@
  *
  * Execution is re-entrant: omp_sse_block.cc calls fftw_execute_dft_r2c on one
  * plan from many OpenMP threads at once, so all scratch lives on the stack.
+ *
+ * KFMM_SHIM_SUM_ORDER=1 in the environment sums every 1-D DFT in reverse
+ * order.  FFTW does not fix its summation order (it depends on the plan it
+ * picks), so the reference's potentials legitimately vary by that much; tests
+ * use the switch to measure the reference's own rounding floor.
  */
 #include <assert.h>
 #include <math.h>
@@ -34,6 +39,18 @@
 #endif
 
 #define SHIM_MAXN 32
+
+#ifndef KFMM_SHIM_ORDER_DEFINED
+#define KFMM_SHIM_ORDER_DEFINED
+static int shim_reverse(void) {
+  static int order = -1; /* read once; concurrent first reads store the same value */
+  if (order < 0) {
+    const char* e = getenv("KFMM_SHIM_SUM_ORDER");
+    order = (e && e[0] == '1') ? 1 : 0;
+  }
+  return order;
+}
+#endif
 
 struct PLAN_S {
   int dir; /* -1: r2c forward, +1: c2r backward */
@@ -101,9 +118,11 @@ SP SNAME(plan_many_dft_c2r)(int rank, const int* n, int howmany, SC* in,
 static void cdft_line(SR* re, SR* im, int stride, int n, const SR* cs,
                       const SR* sn, int sign) {
   SR tr[SHIM_MAXN], ti[SHIM_MAXN];
+  const int rev = shim_reverse();
   for (int k = 0; k < n; ++k) {
     SR ar = 0.0, ai = 0.0;
-    for (int x = 0; x < n; ++x) {
+    for (int xs = 0; xs < n; ++xs) {
+      const int x = rev ? n - 1 - xs : xs;
       int m = (k * x) % n;
       SR c = cs[m], s = sign * sn[m];
       SR xr = re[x * stride], xi = im[x * stride];
@@ -126,12 +145,14 @@ void SNAME(execute_dft_r2c)(const SP p, SR* in, SC* out) {
   SR* im = (SR*)malloc(sizeof(SR) * (size_t)nc);
   assert(re && im);
   /* last dimension: real -> half complex, sign -1 */
+  const int rev = shim_reverse();
   for (int a = 0; a < n0; ++a)
     for (int b = 0; b < n1; ++b) {
       const SR* row = in + ((size_t)a * n1 + b) * n2;
       for (int k = 0; k < h2; ++k) {
         SR ar = 0.0, ai = 0.0;
-        for (int x = 0; x < n2; ++x) {
+        for (int xs = 0; xs < n2; ++xs) {
+          const int x = rev ? n2 - 1 - xs : xs;
           int m = (k * x) % n2;
           ar += row[x] * p->cs[2][m];
           ai -= row[x] * p->sn[2][m];
@@ -184,13 +205,23 @@ void SNAME(execute_dft_c2r)(const SP p, SC* in, SR* out) {
       const SR* yi = im + ((size_t)a * n1 + b) * h2;
       SR* row = out + ((size_t)a * n1 + b) * n2;
       for (int x = 0; x < n2; ++x) {
-        SR acc = yr[0];
         int kmax = (n2 % 2 == 0) ? n2 / 2 - 1 : n2 / 2;
-        for (int k = 1; k <= kmax; ++k) {
-          int m = (k * x) % n2;
-          acc += 2.0 * (yr[k] * p->cs[2][m] - yi[k] * p->sn[2][m]);
+        SR acc;
+        if (!shim_reverse()) {
+          acc = yr[0];
+          for (int k = 1; k <= kmax; ++k) {
+            int m = (k * x) % n2;
+            acc += 2.0 * (yr[k] * p->cs[2][m] - yi[k] * p->sn[2][m]);
+          }
+          if (n2 % 2 == 0) acc += (x % 2 ? -yr[n2 / 2] : yr[n2 / 2]);
+        } else {
+          acc = (n2 % 2 == 0) ? (x % 2 ? -yr[n2 / 2] : yr[n2 / 2]) : 0.0;
+          for (int k = kmax; k >= 1; --k) {
+            int m = (k * x) % n2;
+            acc += 2.0 * (yr[k] * p->cs[2][m] - yi[k] * p->sn[2][m]);
+          }
+          acc += yr[0];
         }
-        if (n2 % 2 == 0) acc += (x % 2 ? -yr[n2 / 2] : yr[n2 / 2]);
         row[x] = acc;
       }
     }

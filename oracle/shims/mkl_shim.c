@@ -1,10 +1,27 @@
 /*
  * Test infrastructure (oracle build only): see mkl.h.
+ *
+ * KFMM_SHIM_SUM_ORDER=1 in the environment makes the matrix-vector products
+ * (DGEMV/SGEMV, the reference's M2M, L2L and check-to-equivalent products,
+ * fmm/vecmatop.cc:14-21) sum their columns in reverse order.  MKL does not
+ * fix that order either (it depends on the build, the CPU and the thread
+ * count), so tests use the switch to measure how far the reference's own
+ * potentials move under a legal reordering.
  */
 #include <assert.h>
 #include <stddef.h>
+#include <stdlib.h>
 
 #include "mkl.h"
+
+static int shim_reverse(void) {
+  static int order = -1; /* read once; concurrent first reads store the same value */
+  if (order < 0) {
+    const char* e = getenv("KFMM_SHIM_SUM_ORDER");
+    order = (e && e[0] == '1') ? 1 : 0;
+  }
+  return order;
+}
 
 /* OpenBLAS (gfortran ABI: hidden string lengths after the argument list) */
 extern void scipy_dgesvd_(const char*, const char*, const int*, const int*, double*,
@@ -34,8 +51,10 @@ void DGEMV(const char* trans, const int* m, const int* n, const double* alpha,
            const double* beta, double* y, const int* incy) {
   assert((*trans == 'N' || *trans == 'n') && *incx == 1 && *incy == 1);
   const int M = *m, N = *n, LD = *lda;
+  const int rev = shim_reverse();
   for (int i = 0; i < M; ++i) y[i] *= *beta;
-  for (int j = 0; j < N; ++j) {
+  for (int js = 0; js < N; ++js) {
+    const int j = rev ? N - 1 - js : js;
     const double t = *alpha * x[j];
     const double* col = a + (size_t)j * LD;
     for (int i = 0; i < M; ++i) y[i] += t * col[i];
@@ -72,8 +91,10 @@ void SGEMV(const char* trans, const int* m, const int* n, const float* alpha, co
            const int* incy) {
   assert((*trans == 'N' || *trans == 'n') && *incx == 1 && *incy == 1);
   const int M = *m, N = *n, LD = *lda;
+  const int rev = shim_reverse();
   for (int i = 0; i < M; ++i) y[i] *= *beta;
-  for (int j = 0; j < N; ++j) {
+  for (int js = 0; js < N; ++js) {
+    const int j = rev ? N - 1 - js : js;
     const float t = *alpha * x[j];
     const float* col = a + (size_t)j * LD;
     for (int i = 0; i < M; ++i) y[i] += t * col[i];

@@ -46,8 +46,13 @@ def reference_env(**kw):
 
 
 def run_reference(n, dist, ppb, np_, out_path, coincide=0, nv=100, variant="omp",
-                  tree_only=False, threads=None):
+                  tree_only=False, threads=None, reverse_sums=False):
+    """reverse_sums: the oracle build's FFTW and MKL stand-ins sum in reverse
+    order (KFMM_SHIM_SUM_ORDER=1), a legal reordering those libraries do not
+    rule out; the distance between the two runs is the reference's own FP64
+    rounding floor."""
     env = reference_env(NP=str(np_), C=str(coincide), NV=str(nv))
+    env["KFMM_SHIM_SUM_ORDER"] = "1" if reverse_sums else "0"
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
     cmd = [harness(variant), str(n), dist, str(ppb), out_path] + (["tree"] if tree_only else [])

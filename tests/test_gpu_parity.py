@@ -4,15 +4,20 @@ build) on the same tree, points and operators, phase by phase and end to end,
 and against the reference CPU build itself where oracle/_ref is present.
 
 Tolerances (plain FP64 path):
-  potentials  : max over targets of |phi_gpu - phi_oracle| / |phi_oracle| (for
-                the signed-density ellipsoid, / max|phi_oracle|: per-target
-                relative error is not defined where the potential crosses
-                zero) <= max(1e-12, 2 * floor), where floor is the same measure
-                between the oracle and the oracle with every sum taken in
-                reverse order.  The floor is the algorithm's own FP64 rounding
-                level: the check-to-equivalent pseudo-inverses amplify any
-                reordering by up to their condition number 0.1^-(np+1); it is
-                below 1e-12 for NP <= 4 and ~6e-11 at NP = 6.
+  potentials  : max over targets of |phi_gpu - phi_ref| / |phi_ref| (for the
+                signed-density ellipsoid, / max|phi_ref|: per-target relative
+                error is not defined where the potential crosses zero)
+                <= max(1e-12, 2 * floor).  Against the reference build, floor
+                is the same measure between two runs of the reference itself
+                whose only difference is the summation order inside the
+                third-party routines it calls (FFTW's transforms, MKL's
+                matrix-vector products; KFMM_SHIM_SUM_ORDER), which those
+                libraries leave open.  Against the oracle, floor is the oracle
+                vs itself with every sum reversed.  Either floor is the
+                algorithm's own FP64 rounding level: the check-to-equivalent
+                pseudo-inverses amplify any reordering by up to their condition
+                number 0.1^-(np+1); it is below 1e-12 for NP <= 4 and ~5e-11
+                to 7e-11 at NP = 6.
   per-node expansions: max|d| <= 50 eps kappa * max|ref| per node, kappa =
                 0.1^-(np+1) the pseudo-inverse's condition bound: a rounding
                 difference in a check potential reaches the equivalent density
@@ -37,6 +42,9 @@ CASES = [
     ("ellipseUniformAngles", 6000, 16, 8, 0),
     ("uniform", 65536, 128, 4, 1),  # the CPU-runnable benchmark configuration (fmmd--omp)
 ]
+# the metric's NP and leaf size (512 per box) at a size the reference runs in
+# seconds: depth 3-4 adaptive tree, V lists at depths 2-4, W and X lists
+REF_CASES = CASES + [("uniform", 262144, 512, 6, 0)]
 
 
 def _ids(c):
@@ -89,16 +97,19 @@ def test_plain_fp64_vs_oracle(K, oracle_mod, cuda_ok, case):
 
 @pytest.mark.gpu
 @pytest.mark.skipif(not have_reference_build(), reason="oracle/_ref not built")
-@pytest.mark.parametrize("case", CASES, ids=_ids)
+@pytest.mark.parametrize("case", REF_CASES, ids=_ids)
 def test_plain_fp64_vs_reference_build(K, oracle_mod, cuda_ok, case):
     """End to end against fmmd--omp itself, run here from oracle/_ref.  With
     the reference's own operator matrices handed to the plan (as the drop-in
-    preproc does) the potentials agree to 1e-12 per target; with this
-    library's own pseudo-inverses (one-sided Jacobi instead of LAPACK DGESVD)
-    they agree to the SVD's rounding times kappa."""
+    preproc does) the potentials agree to 1e-12 per target (NP <= 4), or to
+    twice the reference's own reordering floor (NP >= 5); with this library's
+    own pseudo-inverses (one-sided Jacobi instead of LAPACK DGESVD) they agree
+    to the SVD's rounding times kappa."""
     dist, n, ppb, np_, coincide = case
     with tempfile.TemporaryDirectory() as td:
         R = run_reference(n, dist, ppb, np_, os.path.join(td, "r.bin"), coincide, nv=200)
+        R2 = run_reference(n, dist, ppb, np_, os.path.join(td, "r2.bin"), coincide, nv=200,
+                           reverse_sums=True)
     pts = {k: R[k] for k in ("sx", "sy", "sz", "den", "tx", "ty", "tz")}
     tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], ppb)
     for k in ("child", "tag", "src_perm", "trg_perm", "u_idx", "v_idx", "w_idx", "x_idx"):
@@ -111,11 +122,9 @@ def test_plain_fp64_vs_reference_build(K, oracle_mod, cuda_ok, case):
     plan = K.Plan(tree, np_, K.PLAIN_FP64)
     pot_own = plan.evaluate(pts)
     e_own_ops = _pot_err(pot_own, R["pot"], signed)
-    tree_arrays = {k: R[k] for k in oracle_mod.TREE_FIELDS}
-    floor = _pot_err(oracle_mod.evaluate_reordered(tree_arrays, np_, oracle_mod.ops_from_dump(R),
-                                                   pts), R["pot"], signed)
+    floor = _pot_err(R2["pot"], R["pot"], signed)  # the reference's own floor
     print(f"{_ids(case)}: vs reference build: {e_same_ops:.2e} (reference operators), "
-          f"{e_own_ops:.2e} (own operators), floor {floor:.2e}")
+          f"{e_own_ops:.2e} (own operators), reference reordering floor {floor:.2e}")
     assert e_same_ops <= max(1e-12, 2 * floor)
     assert e_own_ops <= max(1e-12, 5 * floor)
     # the reference's own check, rel-L2 against the exact direct sum: no worse
