@@ -114,7 +114,7 @@ def config_of(n):
     the same points, NP and leaf size)."""
     return {"workload": WORKLOAD, "n_points": n, "np": NP, "pts_per_box": PPB,
             "distribution": DIST, "parallelism": "single",
-            "l2": "inputs larger than L2 (points 268 MB; expansions and spectra >1 GB)"}
+            "l2": "inputs > L2 (points 268 MB, spectra 1.2 GB)"}
 
 
 class ClockSampler:
@@ -225,10 +225,8 @@ def run_reference_cpu(n, max_steps, warmup, budget_s):
     return {"value": n / (t - pre) / 1e6, "unit": "Mpts/s", "cores": cores, "kind": "reference",
             "runs": len(times), "seconds": times, "precompute_s": pre,
             "value_with_precompute": n / t / 1e6,
-            "sample": f"fmmd--omp_sse_block {n} {DIST} {PPB} (the full workload), NP={NP}, "
-                      f"OMP_NUM_THREADS={cores} pinned; median 'Total Execution Time' of "
-                      f"{len(times)} runs minus the in-phase operator precompute (a {small}-point "
-                      "run)"}
+            "sample": f"fmmd--omp_sse_block {n} {DIST} {PPB} NP={NP}, {cores} threads; median "
+                      f"Total Execution Time of {len(times)} runs - precompute"}
 
 
 def reference_arm(args):
@@ -351,24 +349,24 @@ def phase_rooflines(K, st, kern_mixed, pipes, hbm_gbs):
         bound_s += bound_t
 
     nf = st["u_pairs"] / (ms["near_field"] * 1e-3)
-    put("near_field", ms["near_field"], nf / 1e12, mufu / 1e12, "Tpairs/s (MUFU rsqrt)",
+    put("near_field", ms["near_field"], nf / 1e12, mufu / 1e12, "Tpair/s MUFU",
         st["u_pairs"] / mufu)
     s2m = st["s2m_pairs"] / max(ms["s2m"] * 1e-3, 1e-9)
-    put("s2m", ms["s2m"], s2m / 1e12, mufu / 1e12, "Tpairs/s (MUFU rsqrt)", st["s2m_pairs"] / mufu)
+    put("s2m", ms["s2m"], s2m / 1e12, mufu / 1e12, "Tpair/s MUFU", st["s2m_pairs"] / mufu)
     gemm_s = (ms["up_gemm"] + ms["down_gemm"]) * 1e-3
     put("level_gemms", ms["up_gemm"] + ms["down_gemm"], st["gemm_flops"] / gemm_s / 1e12,
-        dmma / 1e12, "TFLOP/s (FP64 DMMA)", st["gemm_flops"] / dmma)
+        dmma / 1e12, "TF/s DMMA", st["gemm_flops"] / dmma)
     # V list against HBM: each kernel's compulsory bytes (spectra as complex
     # FP32, one pass; the FFTs also read or write the P-value surfaces)
     half = nspec / 2.0
     b_fft = half * fpad * 8.0 + st["num_nodes"] * P * 8.0
     b_had = 2.0 * half * fpad * 8.0
     for name, b in (("fft_src", b_fft), ("ifft_trg", b_fft)):
-        put(name, ms[name], b / (ms[name] * 1e-3) / 1e9, hbm_gbs, "GB/s (HBM)", b / hbm)
+        put(name, ms[name], b / (ms[name] * 1e-3) / 1e9, hbm_gbs, "GB/s HBM", b / hbm)
     had_flops = st["hadamard_cmacs"] * FLOPS_PER_CMAC
     out["hadamard"] = {"ms": ms["hadamard"],
                        "achieved": b_had / (ms["hadamard"] * 1e-3) / 1e9, "peak": hbm_gbs,
-                       "unit": "GB/s (HBM)", "frac": b_had / (ms["hadamard"] * 1e-3) / hbm,
+                       "unit": "GB/s HBM", "frac": b_had / (ms["hadamard"] * 1e-3) / hbm,
                        "fma_frac": had_flops / (ms["hadamard"] * 1e-3) / fma32}
     bound_s += max(b_had / hbm, had_flops / fma32)
     total_ms = sum(ms.values())
@@ -481,14 +479,14 @@ def main():
     def roof(name, nf_ms):
         rate = pairs / (nf_ms * 1e-3)
         ceil = pipes["fp32_rsqrt_tops" if name == "mixed" else "fp64_rsqrt_tops"] * 1e12
+        # 11 flops per pair (fmm/driver.cc:60) x pairs per launch / launch time;
+        # peak = one pair per measured reciprocal square root
         return {"bound": "fp32 rsqrt (MUFU)" if name == "mixed" else "fp64 rsqrt",
-                "kernel": f"p2p_warp_kernel<{name}> near field (U+W+X+L2T)",
+                "kernel": f"p2p_warp_kernel<{name}>",
                 "achieved": FLOPS_PER_PAIR * rate / 1e12, "peak": FLOPS_PER_PAIR * ceil / 1e12,
                 "unit": "TFLOP/s", "frac": rate / ceil,
                 "traffic": NEAR_FIELD_DRAM_BYTES[name] if n == N_POINTS else None,
                 "algorithmic_bytes": 32.0 * n + 32.0 * n + 8.0 * n + 8.0 * st["num_nodes"] * st["P"],
-                "algorithmic": f"{FLOPS_PER_PAIR:g} flops/pair (fmm/driver.cc:60) x {pairs:.4e} "
-                               "pairs/launch; peak = 1 pair per measured rsqrt",
                 "launch_ms": nf_ms}
 
     batched_res = None
@@ -510,7 +508,6 @@ def main():
     ms_fp64, ph_fp64, kern_fp64, nf_fp64 = res["fp64"]
     rl = roof("mixed", nf_mixed)
     rl["phases"] = phase_rooflines(K, st, kern_mixed, pipes, hbm_gbs)
-    rl["peak_source"] = "kfmm_measure_peak micro-benchmarks (this run); HBM from MEASURED_PEAKS.json"
     line = {
         "metric": METRIC, "value": aggregate_mpts(n, world, ms_mixed), "unit": "Mpts/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed,

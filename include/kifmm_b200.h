@@ -125,6 +125,28 @@ typedef struct {
 kfmm_status kfmm_plan_create_with_operators(const kfmm_tree_desc* tree, int np,
                                             kfmm_precision precision,
                                             const kfmm_operator_set* ops, kfmm_plan** out);
+
+/* Kernel launch choices (no reference counterpart; the reference fixes its
+ * thread-block sizes at compile time, fmm/cuda.cu:35-105).  0 in a field
+ * keeps the plan's own choice.  The autotuner sweeps them.
+ *   nf_blocks   mixed near field compiled for 5 or 6 resident blocks per SM
+ *               (automatic: 5 when W-list surfaces carry > 1% of the pairs)
+ *   job_rows    P2P jobs of at most 32 * job_rows targets, 1..6 (automatic 6)
+ *   had_windows mixed Hadamard: sibling windows per warp of a CTA, 1..8
+ *               (automatic: the shortest span in waves of one CTA per SM)
+ *   splitk_max  level products: largest split-K factor (automatic: K / 64) */
+typedef struct {
+  int nf_blocks;
+  int job_rows;
+  int had_windows;
+  int splitk_max;
+} kfmm_tuning;
+
+/* kfmm_plan_create_with_operators with launch choices; ops and tuning may be
+ * NULL. */
+kfmm_status kfmm_plan_create_tuned(const kfmm_tree_desc* tree, int np, kfmm_precision precision,
+                                   const kfmm_operator_set* ops, const kfmm_tuning* tuning,
+                                   kfmm_plan** out);
 kfmm_status kfmm_plan_destroy(kfmm_plan* plan);
 
 /* Points in ORIGINAL order.  Host variants copy host->device inside the call

@@ -44,6 +44,12 @@ class OperatorSet(ctypes.Structure):
     _fields_ = [(n, _f64p) for n in ("uc2ue", "ue2uc", "dc2de", "de2dc", "ue2dc")]
 
 
+class Tuning(ctypes.Structure):
+    """kfmm_tuning: launch choices, 0 = the plan's automatic choice."""
+    _fields_ = [(n, ctypes.c_int) for n in ("nf_blocks", "job_rows", "had_windows",
+                                             "splitk_max")]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in ("u_pairs", "s2m_pairs", "s2l_pairs", "v_pairs",
                                                 "hadamard_cmacs", "gemm_flops",
@@ -72,6 +78,8 @@ def lib():
         "kfmm_plan_create": [ctypes.POINTER(TreeDesc), i, i, ctypes.POINTER(vp)],
         "kfmm_plan_create_with_operators": [ctypes.POINTER(TreeDesc), i, i,
                                             ctypes.POINTER(OperatorSet), ctypes.POINTER(vp)],
+        "kfmm_plan_create_tuned": [ctypes.POINTER(TreeDesc), i, i, ctypes.POINTER(OperatorSet),
+                                   ctypes.POINTER(Tuning), ctypes.POINTER(vp)],
         "kfmm_plan_destroy": [vp],
         "kfmm_set_sources": [vp, _f64p, _f64p, _f64p, _f64p, vp],
         "kfmm_set_targets": [vp, _f64p, _f64p, _f64p, vp],
@@ -214,24 +222,24 @@ class Tree:
 class Plan:
     """An evaluation plan on the current CUDA device."""
 
-    def __init__(self, tree, np_, precision=PLAIN_FP64, operators=None):
+    def __init__(self, tree, np_, precision=PLAIN_FP64, operators=None, tuning=None):
         """operators: optional dict (uc2ue, ue2uc, dc2de, de2dc[, ue2dc]) in
-        kfmm_operators layout, e.g. the reference's own matrices."""
+        kfmm_operators layout, e.g. the reference's own matrices.  tuning:
+        optional dict of kfmm_tuning fields (launch choices)."""
         self.tree = tree
         self.np = np_
         h = ctypes.c_void_p()
-        if operators is None:
-            check(lib().kfmm_plan_create(ctypes.byref(tree.desc), np_, precision,
-                                         ctypes.byref(h)), "plan_create")
-        else:
-            keep = {k: np.ascontiguousarray(operators[k], np.float64)
-                    for k in ("uc2ue", "ue2uc", "dc2de", "de2dc", "ue2dc") if k in operators}
+        ops = None
+        if operators is not None:
+            self._ops = {k: np.ascontiguousarray(operators[k], np.float64)
+                         for k in ("uc2ue", "ue2uc", "dc2de", "de2dc", "ue2dc") if k in operators}
             null = ctypes.cast(None, _f64p)
-            ops = OperatorSet(*[_p(keep[k]) if k in keep else null
-                                for k in ("uc2ue", "ue2uc", "dc2de", "de2dc", "ue2dc")])
-            check(lib().kfmm_plan_create_with_operators(ctypes.byref(tree.desc), np_, precision,
-                                                        ctypes.byref(ops), ctypes.byref(h)),
-                  "plan_create_with_operators")
+            ops = ctypes.byref(OperatorSet(*[_p(self._ops[k]) if k in self._ops else null
+                                             for k in ("uc2ue", "ue2uc", "dc2de", "de2dc",
+                                                       "ue2dc")]))
+        tune = ctypes.byref(Tuning(**{k: int(v) for k, v in tuning.items()})) if tuning else None
+        check(lib().kfmm_plan_create_tuned(ctypes.byref(tree.desc), np_, precision, ops, tune,
+                                           ctypes.byref(h)), "plan_create")
         self.handle = h
         self.nt = tree.desc.num_trg
         self.ns = tree.desc.num_src

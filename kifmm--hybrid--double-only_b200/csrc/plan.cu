@@ -108,6 +108,7 @@ struct kfmm_plan {
   int had32_groups_per_block = 0;
   int p2p_grid = 0;            // resident P2P blocks on the device
   bool nf_minb5 = false;       // mixed near field with 5 resident blocks per SM
+  kfmm_tuning tune{};          // launch choices asked for at creation (0 = automatic)
   int p2p_grid5 = 0;
   std::vector<GemmBatch> up_gemms, down_gemms;
   int *fft_nodes = nullptr, *ifft_nodes = nullptr;
@@ -204,7 +205,8 @@ kfmm_status add_gemm(kfmm_plan* p, std::vector<GemmBatch>& out, const double* A,
   g.ksplit = (K + kGemmBK - 1) / kGemmBK * kGemmBK;
   if (blocks < want) {
     double best = 1e300;
-    for (int s = 1; s <= std::max(1, K / 64); ++s) {
+    const int smax = p->tune.splitk_max > 0 ? p->tune.splitk_max : std::max(1, K / 64);
+    for (int s = 1; s <= smax; ++s) {
       const int ks = ((K + s - 1) / s + kGemmBK - 1) / kGemmBK * kGemmBK;
       const int ns = (K + ks - 1) / ks;
       const double waves = std::ceil((double)blocks * ns / want);
@@ -528,7 +530,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_CUDA(cudaMemset(p->spec, 0, p->cplx * (size_t)nn * p->Fpad));
   KF_CUDA(cudaMemset(p->effv, 0, p->cplx * (size_t)nn * p->Fpad));
 
-  const int chunk = 32 * kMaxSlots;
+  const int chunk = 32 * (p->tune.job_rows > 0 ? std::min(p->tune.job_rows, kMaxSlots) : kMaxSlots);
   auto add_chunks = [&](std::vector<P2PJob>& jobs, int tnode, int tkind, int tbeg0, int tcount,
                         int ebeg, int eend, int out0, int mode) {
     for (int c = 0; c < tcount; c += chunk) {
@@ -807,7 +809,9 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     }
     order_jobs(jobs, ent, &p->nf_class);
     p->n_nf = (int)jobs.size();
-    p->nf_minb5 = p->prec == KFMM_MIXED && w_pairs > 0.01 * p->stats.u_pairs;
+    p->nf_minb5 = p->prec == KFMM_MIXED && (p->tune.nf_blocks == 5 ||
+                                            (p->tune.nf_blocks == 0 &&
+                                             w_pairs > 0.01 * p->stats.u_pairs));
     KF_TRY(upload(p, &p->nf_jobs, jobs));
     KF_TRY(upload(p, &p->nf_ent, ent));
   }
@@ -826,6 +830,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     // standing for a CTA's translation-tile load.
     const int nfb = p->Fpad / kFB;
     auto per_block = [&](int items, int warps) {
+      if (p->tune.had_windows > 0) return warps * std::min(p->tune.had_windows, 8);
       int pick = warps;
       double best = 1e300;
       for (int k = 1; k <= 8; ++k) {
@@ -964,6 +969,12 @@ kfmm_status kfmm_plan_create(const kfmm_tree_desc* tree, int np, kfmm_precision 
 kfmm_status kfmm_plan_create_with_operators(const kfmm_tree_desc* tree, int np,
                                             kfmm_precision precision,
                                             const kfmm_operator_set* ops, kfmm_plan** out) {
+  return kfmm_plan_create_tuned(tree, np, precision, ops, nullptr, out);
+}
+
+kfmm_status kfmm_plan_create_tuned(const kfmm_tree_desc* tree, int np, kfmm_precision precision,
+                                   const kfmm_operator_set* ops, const kfmm_tuning* tuning,
+                                   kfmm_plan** out) {
   if (!out) {
     set_error("kfmm_plan_create: out is NULL");
     return KFMM_ERR_INVALID;
@@ -978,9 +989,17 @@ kfmm_status kfmm_plan_create_with_operators(const kfmm_tree_desc* tree, int np,
     return KFMM_ERR_INVALID;
   }
   KF_TRY(validate_desc(tree));
+  if (tuning && (tuning->nf_blocks < 0 || tuning->nf_blocks > 6 ||
+                 (tuning->nf_blocks > 0 && tuning->nf_blocks < 5) || tuning->job_rows < 0 ||
+                 tuning->job_rows > kMaxSlots || tuning->had_windows < 0 ||
+                 tuning->had_windows > 8 || tuning->splitk_max < 0)) {
+    set_error("kfmm_plan_create_tuned: tuning value out of range");
+    return KFMM_ERR_INVALID;
+  }
   kfmm_plan* p = new kfmm_plan();
   p->np = np;
   p->prec = precision;
+  if (tuning) p->tune = *tuning;
   kfmm_status s = build_plan(p, tree, ops);
   if (s != KFMM_OK) {
     std::string keep = g_error;
