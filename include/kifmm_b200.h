@@ -193,10 +193,29 @@ kfmm_status kfmm_get_potentials_device(kfmm_plan* plan, double* pot_dev, void* s
  * without a fault (the copy still lands before the kernel exits). */
 kfmm_status kfmm_set_wait_limit(kfmm_plan* plan, long long tries);
 
-/* End-to-end: host inputs (original order) -> host potentials. */
+/* End-to-end: host inputs (original order) -> host potentials
+ * (synchronous; kfmm_evaluate_async followed by kfmm_evaluate_wait). */
 kfmm_status kfmm_evaluate(kfmm_plan* plan, const double* sx, const double* sy,
                           const double* sz, const double* den, const double* tx,
                           const double* ty, const double* tz, double* pot, void* stream);
+
+/* The same, queued without waiting (no reference counterpart: the reference
+ * runs one synchronous solve per process).  The solve runs on `stream`, after
+ * the work already queued there; the host->device copies run on a copy stream
+ * of the plan and the potentials' device->host copy on another, so with
+ * pinned host arrays the copies of one call overlap the solve of the previous
+ * one: back-to-back calls are bounded by the larger of the device time and
+ * the transfer time, not their sum.  The host arrays must stay unchanged, and
+ * `pot` unread, until the call has completed: kfmm_evaluate_join makes
+ * `stream` wait for every call queued on the plan (without blocking the
+ * host), kfmm_evaluate_wait blocks until then and reports KFMM_ERR_CUDA if any
+ * of those solves gave up a bounded wait.  Calls on one plan are not
+ * re-entrant; queue them from one host thread on one stream. */
+kfmm_status kfmm_evaluate_async(kfmm_plan* plan, const double* sx, const double* sy,
+                                const double* sz, const double* den, const double* tx,
+                                const double* ty, const double* tz, double* pot, void* stream);
+kfmm_status kfmm_evaluate_join(kfmm_plan* plan, void* stream);
+kfmm_status kfmm_evaluate_wait(kfmm_plan* plan, void* stream);
 
 /* ulist__direct_evaluation (fmm/evaluate.h:27): pot[i] += sum_j den[j] /
  * (4 pi |t_i - s_j|), skipping r == 0.  Device pointers, FP64. */

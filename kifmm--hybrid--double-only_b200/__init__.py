@@ -94,6 +94,9 @@ def lib():
         "kfmm_copy_trg_val": [vp, _f64p, vp],
         "kfmm_get_potentials_device": [vp, vp, vp],
         "kfmm_evaluate": [vp] + [_f64p] * 8 + [vp],
+        "kfmm_evaluate_async": [vp] + [_f64p] * 8 + [vp],
+        "kfmm_evaluate_join": [vp, vp],
+        "kfmm_evaluate_wait": [vp, vp],
         "kfmm_direct_evaluation": [i, vp, vp, vp, vp, i, vp, vp, vp, vp, vp],
         "kfmm_read_array": [vp, i, _f64p, ctypes.c_size_t],
         "kfmm_plan_stats": [vp, ctypes.POINTER(Stats)],

@@ -248,97 +248,48 @@ __device__ __forceinline__ float pair_term1(float tx, float ty, float tz, float 
   return out;
 }
 
-// Compensated FP32 accumulation (two-sum, Knuth): (hi, lo) += b with the
-// rounding error of hi + b kept in lo; on both halves of packed registers.
-__device__ __forceinline__ void two_sum2(unsigned long long& hi, unsigned long long& lo,
-                                         unsigned long long b) {
-  asm("{\n"
-      " .reg .b64 s, bv, av;\n"
-      " add.rn.f32x2 s, %0, %2;\n"   // s  = hi + b
-      " sub.rn.f32x2 bv, s, %0;\n"   // bv = s - hi
-      " sub.rn.f32x2 av, s, bv;\n"   // av = s - bv
-      " sub.rn.f32x2 av, %0, av;\n"  // hi - av
-      " sub.rn.f32x2 bv, %2, bv;\n"  // b - bv
-      " add.rn.f32x2 av, av, bv;\n"  // the rounding error of s
-      " add.rn.f32x2 %1, %1, av;\n"  // lo += error
-      " mov.b64 %0, s;\n"
-      "}\n"
-      : "+l"(hi), "+l"(lo)
-      : "l"(b));
-}
-__device__ __forceinline__ void two_sum1(float& hi, float& lo, float b) {
-  const float s = __fadd_rn(hi, b);
-  const float bv = __fsub_rn(s, hi);
-  const float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bv)), __fsub_rn(b, bv));
-  lo = __fadd_rn(lo, e);
-  hi = s;
-}
-
-// Per-lane state of a mixed row job.  NF full slots: slot k of lane l is
-// target l + 32k, two slots per packed register (the high half of the last
-// register unused when NF is odd, that slot then runs as a scalar).  With
-// kSplit, one more "split" slot holds target 32 NF + (l mod 16) in both half
-// warps: a last row of at most 16 targets is shared by the two half warps,
-// each taking half of every chunk's sources, instead of leaving 16 or more
-// lanes of a 32-wide row idle.  Sums: FP32 over one chunk of sources, then
-// two-sum into (hi, lo), converted to FP64 once at the end of the job.
-template <int NF, bool kSplit>
-struct MixedLane {
-  static constexpr int NP2 = NF / 2, ODD = NF & 1, NPK = (NF + 1) / 2 > 0 ? (NF + 1) / 2 : 1;
-  unsigned long long tx[NPK], ty[NPK], tz[NPK];
-  unsigned long long hi[NPK], lo[NPK];
-  float sx, sy, sz, shi, slo;  // split slot
-};
-
-// One chunk: cnt <= 32 sources staged as described at warp_job_mixed, h =
-// ceil(cnt / 2) steps; step u meets sources u and u + h (positions 2u, 2u+1)
-// in every full slot and, in the split slot, source u (lower half warp) or
-// u + h (upper half warp).  kFull: cnt == 32, 16 steps.
-template <int NF, bool kSplit, bool kGuard, bool kFull>
-__device__ __forceinline__ void chunk_mixed(MixedLane<NF, kSplit>& L, const ulonglong2* buf,
-                                            int h, int half) {
-  using ML = MixedLane<NF, kSplit>;
-  constexpr int NP2 = ML::NP2, ODD = ML::ODD, NPK = ML::NPK;
-  unsigned long long blk[NPK];
-  float b1 = 0.f, bs = 0.f;
+// NS targets per lane: NS / 2 packed pairs, plus one scalar target when NS is
+// odd (the high half of the last packed register is then unused).  Terms are
+// summed in FP32 over blocks of 32 sources (one chunk); the block sums are
+// accumulated in FP64 (acc), which keeps the long sum close to a compensated
+// FP32 sum and leaves the FP32 pipe to the pair terms.  (The FP32 -> FP64
+// conversions take XU slots beside the reciprocal square roots: blocks of 16
+// measured 0.11 ms slower at 4M points, with a 2% smaller rel-L2 error.)
+// buf: per source {x,x},{y,y} then {z,z},{w,w} (two ulonglong2 per source).
+template <int NS, bool kGuard>
+__device__ __forceinline__ void pairs_mixed(const unsigned long long (&tx)[(NS + 1) / 2],
+                                            const unsigned long long (&ty)[(NS + 1) / 2],
+                                            const unsigned long long (&tz)[(NS + 1) / 2],
+                                            double (&acc)[NS], const ulonglong2* buf, int cnt) {
+  constexpr int NP2 = NS / 2, ODD = NS & 1, kBlock = 32;
+  for (int k = 0; k < cnt; k += kBlock) {
+    const int m = min(kBlock, cnt - k);
+    unsigned long long blk[NP2 > 0 ? NP2 : 1];
+    float blk1 = 0.f;
 #pragma unroll
-  for (int t = 0; t < NPK; ++t) blk[t] = 0ull;
-  auto step = [&](int u) {
-    const ulonglong2 a0 = buf[4 * u], a1 = buf[4 * u + 1];
-    const ulonglong2 c0 = buf[4 * u + 2], c1 = buf[4 * u + 3];
+    for (int t = 0; t < NP2; ++t) blk[t] = 0ull;
+    auto step = [&](int u) {
+      const ulonglong2 a = buf[2 * (k + u)], b = buf[2 * (k + u) + 1];
+#pragma unroll
+      for (int t = 0; t < NP2; ++t) blk[t] = pair_term2<kGuard>(tx[t], ty[t], tz[t], a, b, blk[t]);
+      if (ODD)
+        blk1 = pair_term1<kGuard>(lo_of(tx[NP2]), lo_of(ty[NP2]), lo_of(tz[NP2]), lo_of(a.x),
+                                  lo_of(a.y), lo_of(b.x), lo_of(b.y), blk1);
+    };
+    if (m == kBlock) {
+      constexpr int kUnroll = NS > 4 ? 2 : 4;  // bounds the live pair temporaries
+#pragma unroll kUnroll
+      for (int u = 0; u < kBlock; ++u) step(u);
+    } else {
+      for (int u = 0; u < m; ++u) step(u);
+    }
 #pragma unroll
     for (int t = 0; t < NP2; ++t) {
-      blk[t] = pair_term2<kGuard>(L.tx[t], L.ty[t], L.tz[t], a0, a1, blk[t]);
-      blk[t] = pair_term2<kGuard>(L.tx[t], L.ty[t], L.tz[t], c0, c1, blk[t]);
+      acc[2 * t] += (double)lo_of(blk[t]);
+      acc[2 * t + 1] += (double)hi_of(blk[t]);
     }
-    if (ODD) {
-      const float x = lo_of(L.tx[NPK - 1]), y = lo_of(L.ty[NPK - 1]), z = lo_of(L.tz[NPK - 1]);
-      b1 = pair_term1<kGuard>(x, y, z, lo_of(a0.x), lo_of(a0.y), lo_of(a1.x), lo_of(a1.y), b1);
-      b1 = pair_term1<kGuard>(x, y, z, lo_of(c0.x), lo_of(c0.y), lo_of(c1.x), lo_of(c1.y), b1);
-    }
-    if (kSplit) {  // the lower half warp takes source u, the upper one u + h
-      const float x = half ? lo_of(c0.x) : lo_of(a0.x), y = half ? lo_of(c0.y) : lo_of(a0.y);
-      const float z = half ? lo_of(c1.x) : lo_of(a1.x), w = half ? lo_of(c1.y) : lo_of(a1.y);
-      bs = pair_term1<kGuard>(L.sx, L.sy, L.sz, x, y, z, w, bs);
-    }
-  };
-  if (kFull) {
-    constexpr int kUnroll = NF > 3 ? 1 : 2;  // bounds the live pair temporaries
-#pragma unroll kUnroll
-    for (int u = 0; u < 16; ++u) step(u);
-  } else {
-#pragma unroll 1
-    for (int u = 0; u < h; ++u) step(u);
+    if (ODD) acc[NS - 1] += (double)blk1;
   }
-#pragma unroll
-  for (int t = 0; t < NP2; ++t) two_sum2(L.hi[t], L.lo[t], blk[t]);
-  if (ODD) {
-    float h1 = lo_of(L.hi[NPK - 1]), l1 = lo_of(L.lo[NPK - 1]);
-    two_sum1(h1, l1, b1);
-    L.hi[NPK - 1] = pack2(h1, 0.f);
-    L.lo[NPK - 1] = pack2(l1, 0.f);
-  }
-  if (kSplit) two_sum1(L.shi, L.slo, bs);
 }
 
 // Target i of job J (i < J.tcnt), absolute FP64 coordinates.
@@ -396,103 +347,68 @@ struct EntryCursor {
   }
 };
 
-// Mixed form of a row job (see warp-autonomous P2P above), NF full slots and
-// an optional split slot (MixedLane).  Each chunk of cnt <= 32 sources goes
-// through the warp's shared buffer in the target node's FP32 frame: with h =
-// ceil(cnt / 2), source s sits at position 2 (s mod h) + s / h, so step u of
-// the pair loop reads sources u and u + h side by side (and each half warp
-// its own one for the split slot, without bank conflicts); an odd count
-// leaves position 2h - 1 to a null source (far away, zero density) whose
-// terms are exactly zero.  A position is {x,x},{y,y} then {z,z},{w,w}.
-template <int NF, bool kSplit>
+// Mixed form of a row job (see warp-autonomous P2P above): slot k of lane l
+// is target l + 32k; each chunk of 32 sources goes through the warp's shared
+// buffer in the target node's FP32 frame and is read back as broadcasts.
+template <int NS>
 __device__ __forceinline__ void warp_job_mixed(const P2PMixedParams& a, const P2PJob& J, int lane,
                                                void* wbuf) {
-  using ML = MixedLane<NF, kSplit>;
-  constexpr int NPK = ML::NPK;
   const P2PParams& p = a.p;
   const double4 org = p.ctr[J.tnode];
   const float4 orgf = a.ctrf[J.tnode];
-  const int half = lane >> 4;
-  ML L;
+  constexpr int NP2C = (NS + 1) / 2;
+  unsigned long long tx[NP2C], ty[NP2C], tz[NP2C];
   {
-    float q[2 * NPK][3];
+    float q[NS][3];
 #pragma unroll
-    for (int t = 0; t < 2 * NPK; ++t) {
+    for (int t = 0; t < NS; ++t) {
       const int i = lane + 32 * t;
       double3 v = make_double3(org.x, org.y, org.z);
-      if (t < NF && i < J.tcnt) v = job_target(p, J, org, i);
+      if (i < J.tcnt) v = job_target(p, J, org, i);
       q[t][0] = (float)(v.x - org.x);
       q[t][1] = (float)(v.y - org.y);
       q[t][2] = (float)(v.z - org.z);
     }
 #pragma unroll
-    for (int t = 0; t < NPK; ++t) {
-      L.tx[t] = pack2(q[2 * t][0], q[2 * t + 1][0]);
-      L.ty[t] = pack2(q[2 * t][1], q[2 * t + 1][1]);
-      L.tz[t] = pack2(q[2 * t][2], q[2 * t + 1][2]);
-      L.hi[t] = L.lo[t] = 0ull;
-    }
-    L.sx = L.sy = L.sz = L.shi = L.slo = 0.f;
-    if (kSplit) {
-      const int i = 32 * NF + (lane & 15);
-      double3 v = make_double3(org.x, org.y, org.z);
-      if (i < J.tcnt) v = job_target(p, J, org, i);
-      L.sx = (float)(v.x - org.x);
-      L.sy = (float)(v.y - org.y);
-      L.sz = (float)(v.z - org.z);
+    for (int t = 0; t < NP2C; ++t) {
+      const int u = 2 * t + 1 < NS ? 2 * t + 1 : 2 * t;
+      tx[t] = pack2(q[2 * t][0], q[u][0]);
+      ty[t] = pack2(q[2 * t][1], q[u][1]);
+      tz[t] = pack2(q[2 * t][2], q[u][2]);
     }
   }
   EntryCursor c{J.ebeg, J.eend, 0, 0, 0, 0, 0, make_float3(0.f, 0.f, 0.f), 0.f};
   c.open(a, orgf);
   float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
   if (c.e < c.eend && lane < min(32, c.count)) s = c.source(a, lane);
+  double acc[NS];
+#pragma unroll
+  for (int t = 0; t < NS; ++t) acc[t] = 0.0;
   ulonglong2* buf = (ulonglong2*)wbuf;
   while (c.e < c.eend) {
     const int cnt = min(32, c.count - c.c0);
-    const int h = (cnt + 1) >> 1;
     const bool guard = c.kind == 0 && J.tkind == 0 && c.node == J.tnode;
     if (lane < cnt) {
       const float x = s.x + c.dlt.x, y = s.y + c.dlt.y, z = s.z + c.dlt.z;
-      const int pos = lane < h ? 2 * lane : 2 * (lane - h) + 1;
-      buf[2 * pos] = make_ulonglong2(pack2(x, x), pack2(y, y));
-      buf[2 * pos + 1] = make_ulonglong2(pack2(z, z), pack2(s.w, s.w));
-    } else if (lane == cnt && (cnt & 1)) {  // null source at position 2h - 1
-      const float far = 1e10f;
-      buf[2 * (2 * h - 1)] = make_ulonglong2(pack2(far, far), pack2(far, far));
-      buf[2 * (2 * h - 1) + 1] = make_ulonglong2(pack2(far, far), 0ull);
+      buf[2 * lane] = make_ulonglong2(pack2(x, x), pack2(y, y));
+      buf[2 * lane + 1] = make_ulonglong2(pack2(z, z), pack2(s.w, s.w));
     }
     __syncwarp();
     c.advance(a, orgf);
     if (c.e < c.eend && lane < min(32, c.count - c.c0)) s = c.source(a, lane);
-    if (cnt == 32) {
-      if (guard) chunk_mixed<NF, kSplit, true, true>(L, buf, 16, half);
-      else chunk_mixed<NF, kSplit, false, true>(L, buf, 16, half);
-    } else {
-      if (guard) chunk_mixed<NF, kSplit, true, false>(L, buf, h, half);
-      else chunk_mixed<NF, kSplit, false, false>(L, buf, h, half);
-    }
+    if (guard) pairs_mixed<NS, true>(tx, ty, tz, acc, buf, cnt);
+    else pairs_mixed<NS, false>(tx, ty, tz, acc, buf, cnt);
     __syncwarp();
   }
-  double* out = p.out;
-  auto store = [&](int i, double v) {
-    const double r = kOOFP * v;
-    double* o = out + (a.out_perm ? a.out_perm[J.out + i] : J.out + i);
-    if (J.mode) *o += r;
-    else *o = r;
-  };
 #pragma unroll
-  for (int t = 0; t < NPK; ++t) {
-    const int i0 = lane + 64 * t, i1 = i0 + 32;
-    if (2 * t < NF && i0 < J.tcnt)
-      store(i0, (double)lo_of(L.hi[t]) + (double)lo_of(L.lo[t]));
-    if (2 * t + 1 < NF && i1 < J.tcnt)
-      store(i1, (double)hi_of(L.hi[t]) + (double)hi_of(L.lo[t]));
-  }
-  if (kSplit) {
-    double v = (double)L.shi + (double)L.slo;
-    v += __shfl_xor_sync(0xffffffffu, v, 16);
-    const int i = 32 * NF + lane;
-    if (lane < 16 && i < J.tcnt) store(i, v);
+  for (int t = 0; t < NS; ++t) {
+    const int i = lane + 32 * t;
+    if (i < J.tcnt) {
+      const double r = kOOFP * acc[t];
+      double* o = p.out + (a.out_perm ? a.out_perm[J.out + i] : J.out + i);
+      if (J.mode) *o += r;
+      else *o = r;
+    }
   }
 }
 
@@ -578,41 +494,23 @@ __device__ __forceinline__ void warp_job_fp64(const P2PParams& p, const P2PJob& 
   }
 }
 
-// Dispatch on the job's row count: a mixed job whose last row holds at most
-// 16 targets runs that row as a split slot (MixedLane).
+template <bool kMixed, int NS>
+__device__ __forceinline__ void warp_job(const P2PArgs<kMixed>& a, const P2PJob& J, int lane,
+                                         void* wbuf) {
+  if constexpr (kMixed) warp_job_mixed<NS>(a, J, lane, wbuf);
+  else warp_job_fp64<NS>(a, J, lane, wbuf);
+}
+
 template <bool kMixed>
 __device__ __forceinline__ void run_job(const P2PArgs<kMixed>& a, const P2PJob& J, int lane,
                                         void* wb) {
-  const int rows = (J.tcnt + 31) >> 5;
-  if constexpr (kMixed) {
-    if (J.tcnt - 32 * (rows - 1) <= 16) {
-      switch (rows) {
-        case 1: warp_job_mixed<0, true>(a, J, lane, wb); break;
-        case 2: warp_job_mixed<1, true>(a, J, lane, wb); break;
-        case 3: warp_job_mixed<2, true>(a, J, lane, wb); break;
-        case 4: warp_job_mixed<3, true>(a, J, lane, wb); break;
-        case 5: warp_job_mixed<4, true>(a, J, lane, wb); break;
-        default: warp_job_mixed<kMaxSlots - 1, true>(a, J, lane, wb); break;
-      }
-    } else {
-      switch (rows) {
-        case 1: warp_job_mixed<1, false>(a, J, lane, wb); break;
-        case 2: warp_job_mixed<2, false>(a, J, lane, wb); break;
-        case 3: warp_job_mixed<3, false>(a, J, lane, wb); break;
-        case 4: warp_job_mixed<4, false>(a, J, lane, wb); break;
-        case 5: warp_job_mixed<5, false>(a, J, lane, wb); break;
-        default: warp_job_mixed<kMaxSlots, false>(a, J, lane, wb); break;
-      }
-    }
-  } else {
-    switch (rows) {
-      case 1: warp_job_fp64<1>(a, J, lane, wb); break;
-      case 2: warp_job_fp64<2>(a, J, lane, wb); break;
-      case 3: warp_job_fp64<3>(a, J, lane, wb); break;
-      case 4: warp_job_fp64<4>(a, J, lane, wb); break;
-      case 5: warp_job_fp64<5>(a, J, lane, wb); break;
-      default: warp_job_fp64<kMaxSlots>(a, J, lane, wb); break;
-    }
+  switch ((J.tcnt + 31) >> 5) {
+    case 1: warp_job<kMixed, 1>(a, J, lane, wb); break;
+    case 2: warp_job<kMixed, 2>(a, J, lane, wb); break;
+    case 3: warp_job<kMixed, 3>(a, J, lane, wb); break;
+    case 4: warp_job<kMixed, 4>(a, J, lane, wb); break;
+    case 5: warp_job<kMixed, 5>(a, J, lane, wb); break;
+    default: warp_job<kMixed, kMaxSlots>(a, J, lane, wb); break;
   }
 }
 
@@ -639,7 +537,8 @@ p2p_warp_kernel(P2PArgs<kMixed> a, int njobs, int* next_job) {
     if (lane == 0) j = atomicAdd(next_job, 1);
     j = __shfl_sync(0xffffffffu, j, 0);
     if (j >= njobs) return;
-    run_job<kMixed>(a, base_of(a).jobs[j], lane, wb);
+    const P2PJob J = base_of(a).jobs[j];  // a register copy: the output stores may alias
+    run_job<kMixed>(a, J, lane, wb);
   }
 }
 
@@ -657,7 +556,8 @@ p2p_fused_kernel(const P2PArgs<kMixed>* params, const int2* jobs, int njobs, int
     if (j >= njobs) return;
     const int2 pj = jobs[j];
     const P2PArgs<kMixed>& a = params[pj.x];
-    run_job<kMixed>(a, base_of(a).jobs[pj.y], lane, wb);
+    const P2PJob J = base_of(a).jobs[pj.y];
+    run_job<kMixed>(a, J, lane, wb);
   }
 }
 
@@ -1504,6 +1404,12 @@ __global__ void scatter_pot_kernel(int n, const int* perm, const double* pot_lea
                                    double* pot_orig) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     pot_orig[perm[i]] = pot_leaf[i];
+}
+
+// error[1] |= error[0]: the per-solve flag of a bounded wait folded into the
+// flag kfmm_evaluate_wait reports for every solve queued since the last wait.
+__global__ void error_fold_kernel(int* error) {
+  if (error[0]) error[1] = 1;
 }
 
 // Plain direct sum (ulist__direct_evaluation) over SoA device arrays.

@@ -103,7 +103,9 @@ struct kfmm_plan {
   int n_s2m = 0, n_nf = 0, n_s2l = 0;
   std::vector<float> nf_class;  // cost class of each near-field job (-log1.25 cost)
   int* job_counter = nullptr;  // persistent P2P work counters: S2M, S2L, near field
-  int* d_error = nullptr;      // set by kernels whose bounded waits ran out; zeroed per solve
+  // [0] set by kernels whose bounded waits ran out, zeroed per solve; [1]
+  // collects [0] over the kfmm_evaluate_async calls since the last wait
+  int* d_error = nullptr;
   long long wait_limit = kMbarSpinLimit;  // tries of the V-list tile-copy wait
   int had32_groups_per_block = 0;
   int p2p_grid = 0;            // resident P2P blocks on the device
@@ -130,10 +132,13 @@ struct kfmm_plan {
   // 7 down done, 8 near field done, 9 copy done
   static constexpr int kMarks = 10;
   cudaEvent_t ev[kMarks] = {};
-  // kfmm_evaluate uploads the targets on a second stream while the far field
-  // (which needs only the sources) runs
-  cudaStream_t side = nullptr;
-  cudaEvent_t side_done = nullptr, src_done = nullptr;
+  // kfmm_evaluate(_async): host->device copies and the target gather run on
+  // `side`, the potentials' device->host copy on `d2h`, the solve on the
+  // caller's stream; the events order successive solves (see
+  // kfmm_evaluate_async)
+  cudaStream_t side = nullptr, d2h = nullptr;
+  cudaEvent_t ev_h2d_src = nullptr, ev_gsrc = nullptr, ev_gtrg = nullptr, ev_nf = nullptr,
+              ev_d2h = nullptr;
 };
 
 namespace {
@@ -849,8 +854,8 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
 
   if (p->splitk_doubles) KF_TRY(dalloc(p, &p->splitk, p->splitk_doubles));
   KF_TRY(dalloc(p, &p->job_counter, 3));
-  KF_TRY(dalloc(p, &p->d_error, 1));
-  KF_CUDA(cudaMemset(p->d_error, 0, sizeof(int)));
+  KF_TRY(dalloc(p, &p->d_error, 2));
+  KF_CUDA(cudaMemset(p->d_error, 0, 2 * sizeof(int)));
   {
     int occ = 0;
     if (p->prec == KFMM_MIXED)
@@ -882,8 +887,9 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
                       (p->prec == KFMM_MIXED ? 0 : 1);  // the plain form's scatter pass
   for (int i = 0; i < kfmm_plan::kMarks; ++i) KF_CUDA(cudaEventCreate(&p->ev[i]));
   KF_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
-  KF_CUDA(cudaEventCreateWithFlags(&p->side_done, cudaEventDisableTiming));
-  KF_CUDA(cudaEventCreateWithFlags(&p->src_done, cudaEventDisableTiming));
+  KF_CUDA(cudaStreamCreateWithFlags(&p->d2h, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&p->ev_h2d_src, &p->ev_gsrc, &p->ev_gtrg, &p->ev_nf, &p->ev_d2h})
+    KF_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   return KFMM_OK;
 }
 
@@ -1016,9 +1022,10 @@ kfmm_status kfmm_plan_destroy(kfmm_plan* p) {
   for (void* v : p->allocs) cudaFree(v);
   for (int i = 0; i < kfmm_plan::kMarks; ++i)
     if (p->ev[i]) cudaEventDestroy(p->ev[i]);
-  if (p->side_done) cudaEventDestroy(p->side_done);
-  if (p->src_done) cudaEventDestroy(p->src_done);
+  for (cudaEvent_t e : {p->ev_h2d_src, p->ev_gsrc, p->ev_gtrg, p->ev_nf, p->ev_d2h})
+    if (e) cudaEventDestroy(e);
   if (p->side) cudaStreamDestroy(p->side);
+  if (p->d2h) cudaStreamDestroy(p->d2h);
   delete p;
   return KFMM_OK;
 }
@@ -1238,37 +1245,89 @@ kfmm_status kfmm_run(kfmm_plan* p, void* stream) {
   return KFMM_OK;
 }
 
-kfmm_status kfmm_evaluate(kfmm_plan* p, const double* sx, const double* sy, const double* sz,
-                          const double* den, const double* tx, const double* ty,
-                          const double* tz, double* pot, void* stream) {
-  if (!p || !pot) {
-    set_error("kfmm_evaluate: null argument");
+kfmm_status kfmm_evaluate_async(kfmm_plan* p, const double* sx, const double* sy,
+                                const double* sz, const double* den, const double* tx,
+                                const double* ty, const double* tz, double* pot, void* stream) {
+  if (!p || !pot || !sx || !sy || !sz || !den || !tx || !ty || !tz) {
+    set_error("kfmm_evaluate_async: null argument");
     return KFMM_ERR_INVALID;
   }
-  if (!tx || !ty || !tz) {
-    set_error("kfmm_evaluate: null argument");
-    return KFMM_ERR_INVALID;
-  }
-  // Sources first; the far field (up, V, X, down) needs nothing else, so it
-  // is queued on `stream` and the targets are uploaded and gathered on the
-  // plan's side stream meanwhile (after the sources' copy); the near field
-  // waits for them.  With pageable host arrays the target copy blocks this
-  // thread while the queued far field runs.
-  cudaStream_t st = S(stream);
-  KF_TRY(kfmm_set_sources(p, sx, sy, sz, den, stream));
-  // the target copy starts once the sources are in (one transfer at a time)
-  KF_CUDA(cudaEventRecord(p->src_done, st));
-  KF_CUDA(cudaStreamWaitEvent(p->side, p->src_done, 0));
+  // Streams: copies and the target gather on `side`, the solve on `stream`,
+  // the potentials' copy back on `d2h`.  The events keep each buffer's
+  // readers and writers of successive calls in order, and nothing else, so a
+  // call's copies overlap the previous call's solve:
+  //   staging o_s*  : H2D(i) after gather_src(i-1)          (ev_gsrc)
+  //   staging o_t*  : H2D(i) after gather_trg(i-1)          (side order)
+  //   trg4          : gather_trg(i) after near field(i-1)   (ev_nf)
+  //   src4 / src4f  : gather_src(i) after near field(i-1)   (stream order)
+  //   pot_orig      : near field(i) after D2H(i-1)          (ev_d2h)
+  cudaStream_t st = S(stream), sd = p->side;
+  const size_t bs = sizeof(double) * p->ns, bt = sizeof(double) * p->nt;
+  KF_CUDA(cudaStreamWaitEvent(sd, p->ev_gsrc, 0));
+  KF_CUDA(cudaMemcpyAsync(p->o_sx, sx, bs, cudaMemcpyHostToDevice, sd));
+  KF_CUDA(cudaMemcpyAsync(p->o_sy, sy, bs, cudaMemcpyHostToDevice, sd));
+  KF_CUDA(cudaMemcpyAsync(p->o_sz, sz, bs, cudaMemcpyHostToDevice, sd));
+  KF_CUDA(cudaMemcpyAsync(p->o_w, den, bs, cudaMemcpyHostToDevice, sd));
+  KF_CUDA(cudaEventRecord(p->ev_h2d_src, sd));
+  KF_CUDA(cudaMemcpyAsync(p->o_tx, tx, bt, cudaMemcpyHostToDevice, sd));
+  KF_CUDA(cudaMemcpyAsync(p->o_ty, ty, bt, cudaMemcpyHostToDevice, sd));
+  KF_CUDA(cudaMemcpyAsync(p->o_tz, tz, bt, cudaMemcpyHostToDevice, sd));
+  KF_CUDA(cudaStreamWaitEvent(sd, p->ev_nf, 0));
+  KF_TRY(kfmm_set_targets_device(p, p->o_tx, p->o_ty, p->o_tz, sd));
+  KF_CUDA(cudaEventRecord(p->ev_gtrg, sd));
+
+  KF_CUDA(cudaStreamWaitEvent(st, p->ev_h2d_src, 0));
+  KF_TRY(kfmm_set_sources_device(p, p->o_sx, p->o_sy, p->o_sz, p->o_w, stream));
+  KF_CUDA(cudaEventRecord(p->ev_gsrc, st));
   KF_TRY(run_far_field(p, stream));
-  KF_TRY(kfmm_set_targets(p, tx, ty, tz, p->side));
-  KF_CUDA(cudaEventRecord(p->side_done, p->side));
-  KF_CUDA(cudaStreamWaitEvent(st, p->side_done, 0));
+  KF_CUDA(cudaStreamWaitEvent(st, p->ev_gtrg, 0));
+  KF_CUDA(cudaStreamWaitEvent(st, p->ev_d2h, 0));
   KF_TRY(kfmm_ulist_calc(p, stream));
   mark(p, 8, st);
   KF_TRY(kfmm_copy_trg_val(p, nullptr, stream));
   mark(p, 9, st);
-  KF_CUDA(cudaMemcpyAsync(pot, p->pot_orig, sizeof(double) * p->nt, cudaMemcpyDeviceToHost, st));
-  return sync_and_check(p, st);
+  error_fold_kernel<<<1, 1, 0, st>>>(p->d_error);
+  KF_CHECK_LAUNCH("error_fold_kernel");
+  KF_CUDA(cudaEventRecord(p->ev_nf, st));
+
+  KF_CUDA(cudaStreamWaitEvent(p->d2h, p->ev_nf, 0));
+  KF_CUDA(cudaMemcpyAsync(pot, p->pot_orig, bt, cudaMemcpyDeviceToHost, p->d2h));
+  KF_CUDA(cudaEventRecord(p->ev_d2h, p->d2h));
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_evaluate_join(kfmm_plan* p, void* stream) {
+  if (!p) {
+    set_error("kfmm_evaluate_join: null plan");
+    return KFMM_ERR_INVALID;
+  }
+  KF_CUDA(cudaStreamWaitEvent(S(stream), p->ev_d2h, 0));
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_evaluate_wait(kfmm_plan* p, void* stream) {
+  KF_TRY(kfmm_evaluate_join(p, stream));
+  int err[2] = {0, 0};
+  KF_CUDA(cudaMemcpyAsync(err, p->d_error, 2 * sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+  KF_CUDA(cudaStreamSynchronize(S(stream)));
+  if (err[1]) {
+    KF_CUDA(cudaMemsetAsync(p->d_error + 1, 0, sizeof(int), S(stream)));
+    KF_CUDA(cudaStreamSynchronize(S(stream)));
+    set_error("a kernel's bounded wait ran out (V-list translation tile copy)");
+    return KFMM_ERR_CUDA;
+  }
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_evaluate(kfmm_plan* p, const double* sx, const double* sy, const double* sz,
+                          const double* den, const double* tx, const double* ty,
+                          const double* tz, double* pot, void* stream) {
+  if (!p || !pot || !tx || !ty || !tz) {
+    set_error("kfmm_evaluate: null argument");
+    return KFMM_ERR_INVALID;
+  }
+  KF_TRY(kfmm_evaluate_async(p, sx, sy, sz, den, tx, ty, tz, pot, stream));
+  return kfmm_evaluate_wait(p, stream);
 }
 
 kfmm_status kfmm_direct_evaluation(int nt, const double* tx, const double* ty, const double* tz,
@@ -1396,6 +1455,10 @@ kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
     njobs += plans[i]->n_nf;
   }
   fused = fused && njobs > 0 && njobs < (size_t)INT32_MAX;
+  // A single solve is captured as its own launches (its near field keeps the
+  // by-value argument block of the regular kernel).
+  const bool single = nplans == 1;
+  if (single) fused = false;
   if (fused) {
     const bool mixed = plans[0]->prec == KFMM_MIXED;
     std::vector<P2PParams> params(nplans);
@@ -1439,16 +1502,16 @@ kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
       cudaStreamWaitEvent(origin, b->events[k], 0);
     }
   };
-  fork();
+  if (!single) fork();
   kfmm_status st = KFMM_OK;
   for (int i = 0; i < nplans && st == KFMM_OK; ++i) {
     const bool timing = plans[i]->timing;
     plans[i]->timing = false;
-    st = fused ? run_far_field(plans[i], b->streams[i % nstreams])
-               : kfmm_run(plans[i], b->streams[i % nstreams]);
+    cudaStream_t on = single ? origin : b->streams[i % nstreams];
+    st = fused ? run_far_field(plans[i], on) : kfmm_run(plans[i], on);
     plans[i]->timing = timing;
   }
-  join();
+  if (!single) join();
   if (fused && st == KFMM_OK) {
     cudaMemsetAsync(b->d_counter, 0, sizeof(int), origin);
     const int blocks = std::min(plans[0]->p2p_grid,
