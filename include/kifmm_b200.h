@@ -131,7 +131,9 @@ kfmm_status kfmm_plan_create_with_operators(const kfmm_tree_desc* tree, int np,
  * keeps the plan's own choice.  The autotuner sweeps them.
  *   nf_blocks   mixed near field compiled for 5 or 6 resident blocks per SM
  *               (automatic: 5 when W-list surfaces carry > 1% of the pairs)
- *   job_rows    P2P jobs of at most 32 * job_rows targets, 1..6 (automatic 6)
+ *   job_rows    near-field jobs of at most 32 * job_rows targets, 1..6
+ *               (automatic: 4 for mixed plans whose W lists carry > 1% of the
+ *               pairs, else 6)
  *   had_windows mixed Hadamard: sibling windows per warp of a CTA, 1..8
  *               (automatic: the shortest span in waves of one CTA per SM)
  *   splitk_max  level products: largest split-K factor (automatic: K / 64) */

@@ -535,7 +535,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_CUDA(cudaMemset(p->spec, 0, p->cplx * (size_t)nn * p->Fpad));
   KF_CUDA(cudaMemset(p->effv, 0, p->cplx * (size_t)nn * p->Fpad));
 
-  const int chunk = 32 * (p->tune.job_rows > 0 ? std::min(p->tune.job_rows, kMaxSlots) : kMaxSlots);
+  int chunk = 32 * kMaxSlots;  // targets per job (the near field's is chosen below)
   auto add_chunks = [&](std::vector<P2PJob>& jobs, int tnode, int tkind, int tbeg0, int tcount,
                         int ebeg, int eend, int out0, int mode) {
     for (int c = 0; c < tcount; c += chunk) {
@@ -793,7 +793,31 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   {
     std::vector<P2PJob> jobs;
     std::vector<int> ent;
-    double w_pairs = 0.0;  // pairs with W-list UE surfaces
+    // Pairs with W-list UE surfaces: where they carry more than 1% of the
+    // pairs (clouds on surfaces), the mixed near field runs with 5 resident
+    // blocks per SM and jobs of at most 4 rows (128 targets): measured on 4M
+    // points on the ellipsoid surface, NP=4, 256 per box: 2.32 ms against
+    // 2.50 ms with 6 blocks and 6 rows; uniform clouds keep 6 and 6 (4.42 ms,
+    // against 4.70 ms with 4 rows).
+    double w_pairs = 0.0;
+    for (int t = 0; t < nn; ++t) {
+      if (!is_leaf(t) || !has_trg(t) || d->trg_num[t] == 0) continue;
+      for (int k = d->w_ptr[t]; k < d->w_ptr[t + 1]; ++k) {
+        const int s = d->w_idx[k];
+        if (!(is_leaf(s) && d->src_num[s] < P)) w_pairs += (double)d->trg_num[t] * P;
+      }
+    }
+    double all_pairs = 0.0;
+    for (int t = 0; t < nn; ++t) {
+      if (!is_leaf(t) || !has_trg(t)) continue;
+      double ns = 0;
+      for (int k = d->u_ptr[t]; k < d->u_ptr[t + 1]; ++k) ns += d->src_num[d->u_idx[k]];
+      all_pairs += ns * d->trg_num[t];
+    }
+    const bool w_heavy = w_pairs > 0.01 * (all_pairs + w_pairs);
+    int rows = p->prec == KFMM_MIXED && w_heavy ? 4 : kMaxSlots;
+    if (p->tune.job_rows > 0) rows = std::min(p->tune.job_rows, kMaxSlots);
+    chunk = 32 * rows;
     for (int t = 0; t < nn; ++t) {
       if (!is_leaf(t) || !has_trg(t) || d->trg_num[t] == 0) continue;
       int e0 = (int)ent.size();
@@ -802,7 +826,6 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
         int s = d->w_idx[k];
         bool direct = is_leaf(s) && d->src_num[s] < P;  // fmm/omp.cc:675
         ent.push_back(direct ? s : ((1 << 28) | s));
-        if (!direct) w_pairs += (double)d->trg_num[t] * P;
       }
       if (d->trg_num[t] < P)  // fmm/omp.cc:724
         for (int k = d->x_ptr[t]; k < d->x_ptr[t + 1]; ++k) ent.push_back(d->x_idx[k]);
@@ -815,8 +838,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     order_jobs(jobs, ent, &p->nf_class);
     p->n_nf = (int)jobs.size();
     p->nf_minb5 = p->prec == KFMM_MIXED && (p->tune.nf_blocks == 5 ||
-                                            (p->tune.nf_blocks == 0 &&
-                                             w_pairs > 0.01 * p->stats.u_pairs));
+                                            (p->tune.nf_blocks == 0 && w_heavy));
     KF_TRY(upload(p, &p->nf_jobs, jobs));
     KF_TRY(upload(p, &p->nf_ent, ent));
   }
