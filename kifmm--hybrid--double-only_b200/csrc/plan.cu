@@ -118,6 +118,8 @@ struct kfmm_plan {
   int *win = nullptr, *members = nullptr;
   int n_groups = 0;
   // mixed form: x-neighbour pairs of groups and the groups left single
+  unsigned long long* pair_rows = nullptr;  // per pair window: rows holding an entry
+  unsigned long long* single_rows = nullptr;
   int *pair_win = nullptr, *pair_members = nullptr, *single_win = nullptr,
       *single_members = nullptr;
   int n_pairs = 0, n_singles = 0;
@@ -737,6 +739,20 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       p->n_pairs = (int)pmem.size() / 16;
       p->n_singles = (int)smem.size() / 8;
       KF_TRY(upload(p, &p->pair_win, pwin));
+      {
+        std::vector<unsigned long long> prow(pmem.size() / 16, 0ull);
+        for (size_t g = 0; g < prow.size(); ++g)
+          for (int r = 0; r < 36; ++r)
+            for (int x = 0; x < 8; ++x)
+              if (pwin[g * 288 + r * 8 + x] >= 0) prow[g] |= 1ull << r;
+        KF_TRY(upload(p, &p->pair_rows, prow));
+        std::vector<unsigned long long> srow(smem.size() / 8, 0ull);
+        for (size_t g = 0; g < srow.size(); ++g)
+          for (int r = 0; r < 36; ++r)
+            for (int x = 0; x < 6; ++x)
+              if (swin[g * 216 + r * 6 + x] >= 0) srow[g] |= 1ull << r;
+        KF_TRY(upload(p, &p->single_rows, srow));
+      }
       KF_TRY(upload(p, &p->pair_members, pmem));
       KF_TRY(upload(p, &p->single_win, swin));
       KF_TRY(upload(p, &p->single_members, smem));
@@ -1141,7 +1157,7 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
     if (mixed) {
       if (p->n_pairs) {
         const int ppb = p->pair_per_block;
-        HadPairParams h{p->nn, p->n_pairs, ppb, p->pair_win, p->pair_members,
+        HadPairParams h{p->nn, p->n_pairs, ppb, p->pair_win, p->pair_members, p->pair_rows,
                         (const float2*)p->d_trans, (const float2*)p->spec, (float2*)p->effv,
                         p->d_error, p->wait_limit};
         dim3 grid((p->n_pairs + ppb - 1) / ppb, p->Fpad / kFB);
@@ -1150,7 +1166,7 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
       }
       if (p->n_singles) {
         const int gpb = p->had32_groups_per_block;
-        Had32Params h{p->nn, p->n_singles, gpb, p->single_win, p->single_members,
+        Had32Params h{p->nn, p->n_singles, gpb, p->single_win, p->single_members, p->single_rows,
                       (const float2*)p->d_trans, (const float2*)p->spec, (float2*)p->effv,
                       p->d_error, p->wait_limit};
         dim3 grid((p->n_singles + gpb - 1) / gpb, p->Fpad / kFB);
