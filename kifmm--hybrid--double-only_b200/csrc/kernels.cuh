@@ -753,6 +753,86 @@ struct FFTParams {
 constexpr int kFFTThreads = 128;
 constexpr int kMaxNP = 8;
 
+// Multiplication by (-i)^e.
+__device__ __forceinline__ double2 rot_mi(double2 v, int e) {
+  switch (e & 3) {
+    case 0: return v;
+    case 1: return make_double2(v.y, -v.x);
+    case 2: return make_double2(-v.x, -v.y);
+    default: return make_double2(-v.y, v.x);
+  }
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+
+// Pruned forward DFT of length N = 2 NP whose input is non-zero at positions
+// H .. H + NP - 1 only (the surface block, H = NP / 2):
+//   X[q] = sum_k v[k] w^(q (k + H)),  w = exp(-2 pi i / N),  q < N.
+// Decimation in the output index: with Q = NP / 2 (NP even) and q = m + jQ,
+// w^(jQ (k + H)) = (-i)^(j (k + H)) depends on k mod 4 only, so four partial
+// sums per m over k of one residue mod 4 give all four outputs m + jQ:
+// NP * NP / 2 complex multiply-adds instead of 2 NP^2.  For odd NP the split
+// is on q = m + jNP, k mod 2: NP^2.  Twiddles come from the tables cs, sn
+// (cos, sin of 2 pi m / N) at compile-time indices.
+template <int NP>
+__device__ __forceinline__ void dft_fwd_pruned(const double2 (&v)[NP], double2 (&X)[2 * NP],
+                                               const double* cs, const double* sn) {
+  constexpr int N = 2 * NP, H = NP / 2;
+  constexpr int R = NP % 2 == 0 ? 4 : 2, Q = N / R;
+#pragma unroll
+  for (int m = 0; m < Q; ++m) {
+    double2 S[R];
+#pragma unroll
+    for (int c = 0; c < R; ++c) S[c] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      const int e = (m * (k + H)) % N;
+      double2& a = S[k % R];
+      a.x = fma(v[k].x, cs[e], fma(v[k].y, sn[e], a.x));
+      a.y = fma(v[k].y, cs[e], fma(-v[k].x, sn[e], a.y));
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      double2 o = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int c = 0; c < R; ++c) o = cadd(o, rot_mi(S[c], (4 / R) * j * (c + H)));
+      X[m + j * Q] = o;
+    }
+  }
+}
+
+// Pruned inverse DFT of length N = 2 NP evaluated at positions H .. H+NP-1:
+//   y[k] = sum_q X[q] w^(-q (k + H)),  k < NP.
+// With q = m + jQ as above, the inner sum over j only depends on (k + H) mod
+// R: R combinations of the X[m + jQ] per m, then NP * Q multiply-adds.
+template <int NP>
+__device__ __forceinline__ void dft_inv_pruned(const double2 (&X)[2 * NP], double2 (&y)[NP],
+                                               const double* cs, const double* sn) {
+  constexpr int N = 2 * NP, H = NP / 2;
+  constexpr int R = NP % 2 == 0 ? 4 : 2, Q = N / R;
+#pragma unroll
+  for (int k = 0; k < NP; ++k) y[k] = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int m = 0; m < Q; ++m) {
+    double2 T[R];  // T[c] = sum_j X[m + jQ] (+i)^((4/R) j c), c = (k + H) mod R
+#pragma unroll
+    for (int c = 0; c < R; ++c) {
+      double2 o = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int j = 0; j < R; ++j) o = cadd(o, rot_mi(X[m + j * Q], -(4 / R) * j * c));
+      T[c] = o;
+    }
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      const int e = (m * (k + H)) % N;
+      const double2 t = T[(k + H) % R];
+      y[k].x = fma(t.x, cs[e], fma(-t.y, sn[e], y[k].x));
+      y[k].y = fma(t.y, cs[e], fma(t.x, sn[e], y[k].y));
+    }
+  }
+}
+
 // Boxes per block: as many as fit in ~44 KB of static shared memory (at most
 // 3), so that every pass keeps most of the block's threads busy.
 template <int NP>
@@ -828,20 +908,12 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
   for (int q = tid; q < B * NP * NK; q += kFFTThreads) {
     const int bb = q / (NP * NK), t = q % (NP * NK);
     const int k = t / NK, kx = t % NK;
-    double2 v[NP];
+    double2 v[NP], o[N];
 #pragma unroll
     for (int j = 0; j < NP; ++j) v[j] = X[bb][(k * NP + j) * NK + kx];
+    dft_fwd_pruned<NP>(v, o, cs, sn);
 #pragma unroll
-    for (int ky = 0; ky < N; ++ky) {
-      double ar = 0, ai = 0;
-#pragma unroll
-      for (int j = 0; j < NP; ++j) {
-        const int m = (ky * (j + H)) % N;
-        ar = fma(v[j].x, cs[m], fma(v[j].y, sn[m], ar));
-        ai = fma(v[j].y, cs[m], fma(-v[j].x, sn[m], ai));
-      }
-      Y[bb][(k * N + ky) * NK + kx] = make_double2(ar, ai);
-    }
+    for (int ky = 0; ky < N; ++ky) Y[bb][(k * N + ky) * NK + kx] = o[ky];
   }
   __syncthreads();
   // z: column (ky, kx), outputs kz -> spectrum
@@ -851,22 +923,16 @@ __global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
     const int node = node_s[bb];
     if (node < 0) continue;
     const int ky = t / NK, kx = t % NK;
-    double2 v[NP];
+    double2 v[NP], o[N];
 #pragma unroll
     for (int k = 0; k < NP; ++k) v[k] = Y[bb][(k * N + ky) * NK + kx];
+    dft_fwd_pruned<NP>(v, o, cs, sn);
 #pragma unroll
     for (int kz = 0; kz < N; ++kz) {
-      double ar = 0, ai = 0;
-#pragma unroll
-      for (int k = 0; k < NP; ++k) {
-        const int m = (kz * (k + H)) % N;
-        ar = fma(v[k].x, cs[m], fma(v[k].y, sn[m], ar));
-        ai = fma(v[k].y, cs[m], fma(-v[k].x, sn[m], ai));
-      }
-      C o;
-      o.x = ar;
-      o.y = ai;
-      out[spec_index((kz * N + ky) * NK + kx, node, p.nn)] = o;
+      C e;
+      e.x = o[kz].x;
+      e.y = o[kz].y;
+      out[spec_index((kz * N + ky) * NK + kx, node, p.nn)] = e;
     }
   }
 }
@@ -897,20 +963,13 @@ __global__ void __launch_bounds__(kFFTThreads) ifft_trg_np_kernel(FFTParams p) {
     const int node = node_s[bb];
     if (node < 0) continue;
     const int ky = t / NK, kx = t % NK;
-    double2 acc[NP];
-#pragma unroll
-    for (int k = 0; k < NP; ++k) acc[k] = make_double2(0.0, 0.0);
+    double2 v[N], acc[NP];
 #pragma unroll
     for (int kz = 0; kz < N; ++kz) {
       const C e = in[spec_index((kz * N + ky) * NK + kx, node, p.nn)];
-      const double2 v = make_double2(e.x, e.y);
-#pragma unroll
-      for (int k = 0; k < NP; ++k) {
-        const int m = (kz * (k + H)) % N;
-        acc[k].x = fma(v.x, cs[m], fma(-v.y, sn[m], acc[k].x));
-        acc[k].y = fma(v.y, cs[m], fma(v.x, sn[m], acc[k].y));
-      }
+      v[kz] = make_double2(e.x, e.y);
     }
+    dft_inv_pruned<NP>(v, acc, cs, sn);
 #pragma unroll
     for (int k = 0; k < NP; ++k) Z[bb][(k * N + ky) * NK + kx] = acc[k];
   }
@@ -920,19 +979,10 @@ __global__ void __launch_bounds__(kFFTThreads) ifft_trg_np_kernel(FFTParams p) {
     const int bb = q / (NP * NK), t = q % (NP * NK);
     if (node_s[bb] < 0) continue;
     const int k = t / NK, kx = t % NK;
-    double2 acc[NP];
+    double2 v[N], acc[NP];
 #pragma unroll
-    for (int j = 0; j < NP; ++j) acc[j] = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int ky = 0; ky < N; ++ky) {
-      const double2 v = Z[bb][(k * N + ky) * NK + kx];
-#pragma unroll
-      for (int j = 0; j < NP; ++j) {
-        const int m = (ky * (j + H)) % N;
-        acc[j].x = fma(v.x, cs[m], fma(-v.y, sn[m], acc[j].x));
-        acc[j].y = fma(v.y, cs[m], fma(v.x, sn[m], acc[j].y));
-      }
-    }
+    for (int ky = 0; ky < N; ++ky) v[ky] = Z[bb][(k * N + ky) * NK + kx];
+    dft_inv_pruned<NP>(v, acc, cs, sn);
 #pragma unroll
     for (int j = 0; j < NP; ++j) W[bb][(k * NP + j) * NK + kx] = acc[j];
   }
