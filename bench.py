@@ -46,9 +46,13 @@ FLOPS_PER_CMAC = 8.0     # complex multiply-add, fmm/driver.cc:82 (4 * 2F per V 
 NEAR_FIELD_DRAM_BYTES = {"mixed": 533.6e6, "fp64": 610.4e6}
 # batched workload: independent solves, point counts log-uniform in
 # [4096, 262144], half uniform cube / half ellipsoid surface, NP in {3, 4},
-# leaf sizes from the autotuner, all solves in one CUDA graph
+# leaf sizes and launch choices from the autotuner (its table for this
+# workload, tuned on a B200, ships with the package; missing entries are
+# tuned during the run), all solves in one CUDA graph
 BATCH_SOLVES = 256
 BATCH_LEAF_CANDIDATES = (32, 64, 128, 256)
+BATCH_TABLE = os.path.join(ROOT, "kifmm--hybrid--double-only_b200", "tuning_data",
+                           "b200_batched_configs.json")
 # wall-clock budgets of the CPU reference runs (seconds): the timed steps of
 # `--impl reference`, and the cpu_baseline leg of the GPU arm
 REF_ARM_BUDGET_S = 200.0
@@ -298,14 +302,17 @@ def time_batched(K, count, stream, steps, warmup):
     (all solves), Mpts/s, and per-solve distance of the mixed form to the
     plain one."""
     import torch
+    import json as _json
     from kifmm_b200 import autotune, batched
-    autotune.CANDIDATES = BATCH_LEAF_CANDIDATES
     sp = batched.specs(count)
     out = {"solves": count, "points": sum(s["n"] for s in sp)}
     sh = stream.cuda_stream
     pots = {}
+    table = autotune.ConfigTable(candidates=BATCH_LEAF_CANDIDATES)
+    if os.path.exists(BATCH_TABLE):
+        with open(BATCH_TABLE) as f:
+            table.picks = _json.load(f)
     for name, prec in (("mixed", K.MIXED), ("fp64", K.PLAIN_FP64)):
-        table = autotune.LeafSizeTable()
         B = batched.BatchedSolves(K, sp, prec, table=table, nstreams=16)
         for _ in range(warmup):
             B.launch(sh)
@@ -435,6 +442,24 @@ def main():
     clk = clocks.stop()
     pots = {name: pl.potentials(sh) for name, pl in plans.items()}
 
+    # ---- the mixed form replayed as a one-plan batch (one CUDA graph launch
+    # per solve), against the plain form's direct launches
+    graph_ms = {}
+    for name, pl in plans.items():
+        bt = K.Batch([pl], 1)
+        for _ in range(args.warmup):
+            bt.launch(sh)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            bt.launch(sh)
+        b.record(stream)
+        torch.cuda.synchronize()
+        bt.wait(sh)
+        graph_ms[name] = reduce_max(a.elapsed_time(b) / args.steps, world, dev)
+        bt.close()
+
     # ---- the reference's check: rel-L2 vs an FP64 direct sum on 1000 targets
     ids = pts["check_ids"]
     dsrc = [torch.tensor(pts[k], device=dev) for k in ("sx", "sy", "sz", "den")]
@@ -542,6 +567,8 @@ def main():
         "tree": {"nodes": st["num_nodes"], "u_pairs": pairs, "v_pairs": st["v_pairs"],
                  "build_s_host": tree_host_s, "build_s_device": tree_device_s},
         "batched": batched_res,
+        "graph_4m": {"mixed_ms": graph_ms["mixed"], "fp64_ms": graph_ms["fp64"],
+                     "mixed_over_fp64_direct": ms_fp64 / graph_ms["mixed"]},
         "phases_ms": ph_mixed,
         "fp64": {"value": aggregate_mpts(n, world, ms_fp64), "ms_per_step": ms_fp64,
                  "rel_l2_err": err["fp64"], "near_field_frac": roof("fp64", nf_fp64)["frac"],

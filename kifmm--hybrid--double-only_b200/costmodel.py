@@ -1,14 +1,17 @@
-"""Learned cost model for the leaf size (points per box).
+"""Learned cost model for the leaf size (points per box) and the near-field
+kernel's launch choices.
 
 A small network (kfmm_mlp_*: 3 layers, 64 hidden units, FP32, trained and
-evaluated by this library's own CUDA kernels) maps tree statistics to the
-per-phase device times of one solve.  To pick the leaf size of a new cloud,
-the tree is built for every candidate (on the GPU, kfmm_tree_build_device:
-no plan, no solve), the network predicts each candidate's time, and the
-fastest prediction wins.  When the two best predictions are closer than
-`fallback_margin` (10%), those two candidates are measured and the faster
-one is taken: measurement stays the fallback, and the exhaustive measured
-sweep (autotune.best_leaf_size) the yardstick the model is scored against.
+evaluated by this library's own CUDA kernels) maps tree statistics plus a
+near-field configuration (job size in rows of 32 targets, resident blocks
+per SM: CONFIGS) to the per-phase device times of one solve.  To pick for a
+new cloud, the tree is built for every leaf-size candidate (on the GPU,
+kfmm_tree_build_device: no plan, no solve), the network predicts the time of
+every (leaf size, configuration) pair, and the fastest prediction wins.  When
+the two best predictions are closer than `fallback_margin` (10%), those two
+are measured and the faster one is taken: measurement stays the fallback,
+and the exhaustive measured sweep the yardstick the model is scored
+against.
 
 Features of a (cloud, leaf size) tree: log point count, log leaf size, NP,
 node counts per level (16 levels), histograms of the U, V, W and X list
@@ -17,8 +20,13 @@ of U-list point pairs and V, W, X box pairs, and the logs of the work the
 kernels do as the plan counts it: near-field pairs (U + W + direct X + L2T),
 the same padded to the warp's 32-target granularity, S2M and S2L pairs, the
 box, leaf and V-list-box counts, the largest leaf's near-field work and the
-work-weighted histogram of leaf work (8 bins, factors of 4).  Targets: log(ms) of the
-phases up, vlist, xlist, down, ulist (kfmm_phase_times).
+work-weighted histogram of leaf work (8 bins, factors of 4); then the
+configuration (rows per job / 6, 1 for 5 resident blocks).  Targets: log(ms)
+of the phases up, vlist, xlist, down, ulist (kfmm_phase_times).
+
+``harvest`` measures clouds with a pipeline: worker threads build the trees
+(on the host), the features and the plans of the next (cloud, leaf size)
+pairs while the main thread times the ready ones on the GPU, one at a time.
 
 Clouds (``make_cloud``): the uniform cube, the ellipsoid surface, and
 mixtures of 1 to 32 isotropic Gaussian clusters with sigma log-uniform in
@@ -32,6 +40,12 @@ import numpy as np
 
 PHASES = ("up", "vlist", "xlist", "down", "ulist")
 LEAF_SIZES = (32, 64, 128, 256, 512, 1024)
+# near-field launch choices the model ranks (kfmm_tuning fields)
+CONFIGS = ({"job_rows": 6, "nf_blocks": 6}, {"job_rows": 4, "nf_blocks": 5})
+
+
+def config_features(cfg):
+    return [cfg["job_rows"] / 6.0, 1.0 if cfg["nf_blocks"] == 5 else 0.0]
 NLEVELS = 16
 NBINS = 8
 
@@ -76,7 +90,14 @@ def _hist(lengths):
     return h
 
 
-def features(tree, np_, ppb, n):
+def features(tree, np_, ppb, n, cfg=None):
+    """Tree statistics of a (cloud, leaf size) followed by the near-field
+    configuration's features (CONFIGS[0] when cfg is None)."""
+    return np.concatenate([tree_features(tree, np_, ppb, n),
+                           config_features(CONFIGS[0] if cfg is None else cfg)])
+
+
+def tree_features(tree, np_, ppb, n):
     depth = tree.array("depth")
     tag = tree.array("tag")
     src_num = tree.array("src_num").astype(np.float64)
@@ -146,31 +167,44 @@ def features(tree, np_, ppb, n):
     return np.array(f, np.float64)
 
 
-def measure(K, pts, np_, ppb, precision, reps=2, device_tree=True):
-    """Per-phase device ms (minimum over reps after a warm-up) and the tree's
-    features."""
+def time_phases(K, plan, pts, reps=2):
+    """Per-phase device ms of one solve (minimum over reps after a warm-up),
+    the copy phase counted into down."""
+    plan.set_points(pts)
+    plan.run()
+    plan.enable_timing(True)
+    best = None
+    for _ in range(reps):
+        plan.run()
+        ph = plan.phase_times()
+        v = np.array([ph[p] for p in PHASES])
+        v[PHASES.index("down")] += ph["copy"]
+        best = v if best is None else np.minimum(best, v)
+    plan.enable_timing(False)
+    return best
+
+
+def measure(K, pts, np_, ppb, precision, reps=2, device_tree=True, configs=CONFIGS):
+    """The tree's features and, for each configuration, its per-phase ms:
+    [(features, phase ms)] in the order of configs."""
     args = [pts[k] for k in ("sx", "sy", "sz", "tx", "ty", "tz")]
     tree = K.Tree(*args, ppb, device=device_tree)
-    feats = features(tree, np_, ppb, len(pts["sx"]))
-    plan = K.Plan(tree, np_, precision)
     try:
-        plan.set_points(pts)
-        plan.run()
-        plan.enable_timing(True)
-        best = None
-        for _ in range(reps):
-            plan.run()
-            ph = plan.phase_times()
-            v = np.array([ph[p] for p in PHASES])
-            best = v if best is None else np.minimum(best, v)
-        best[PHASES.index("down")] += ph["copy"]
-        return feats, best
+        base = tree_features(tree, np_, ppb, len(pts["sx"]))
+        out = []
+        for cfg in configs:
+            plan = K.Plan(tree, np_, precision, tuning=cfg)
+            try:
+                out.append((np.concatenate([base, config_features(cfg)]),
+                            time_phases(K, plan, pts, reps)))
+            finally:
+                plan.close()
+        return out
     finally:
-        plan.close()
         tree.close()
 
 
-def cloud_specs(count, nmin=65536, nmax=1048576, seed=5):
+def cloud_specs(count, nmin=65536, nmax=8388608, seed=5):
     rng = np.random.default_rng(seed)
     kinds = ("uniform", "ellipsoidSurface", "clusters")
     out = []
@@ -180,24 +214,85 @@ def cloud_specs(count, nmin=65536, nmax=1048576, seed=5):
     return out
 
 
-def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, log=None):
-    """Measured dataset: one row per (cloud, leaf size)."""
+def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, configs=CONFIGS,
+            threads=8, device_bytes=80e9, log=None):
+    """Measured dataset: one row per (cloud, leaf size, configuration).
+    `threads` workers build host trees, features and plans ahead of the
+    timing loop; at most `device_bytes` of plans (estimated at 600 bytes a
+    point each) are held at once."""
+    import queue
+    import threading
     precision = K.MIXED if precision is None else precision
-    rows_f, rows_t, cloud, ppbs = [], [], [], []
-    for ci, sp in enumerate(specs):
-        pts = make_cloud(K, sp["kind"], sp["n"], sp["seed"])
-        for ppb in leaf_sizes:
-            if ppb * 8 > sp["n"]:
-                continue
-            f, t = measure(K, pts, np_, ppb, precision)
-            rows_f.append(f)
-            rows_t.append(t)
+    ready = queue.Queue()
+    held = [0.0]  # estimated device bytes of the plans built and not yet timed
+    room = threading.Condition()
+
+    def reserve(nbytes):
+        with room:
+            room.wait_for(lambda: held[0] == 0.0 or held[0] + nbytes <= device_bytes)
+            held[0] += nbytes
+
+    def release(nbytes):
+        with room:
+            held[0] -= nbytes
+            room.notify_all()
+
+    todo = list(enumerate(specs))
+    todo_lock = threading.Lock()
+    errors = []
+
+    def worker():
+        try:
+            while True:
+                with todo_lock:
+                    if not todo:
+                        return
+                    ci, sp = todo.pop(0)
+                pts = make_cloud(K, sp["kind"], sp["n"], sp["seed"])
+                args = [pts[k] for k in ("sx", "sy", "sz", "tx", "ty", "tz")]
+                for ppb in leaf_sizes:
+                    if ppb * 8 > sp["n"]:
+                        continue
+                    u = 600.0 * sp["n"] * len(configs)
+                    reserve(u)
+                    tree = K.Tree(*args, ppb)
+                    base = tree_features(tree, np_, ppb, sp["n"])
+                    plans = [K.Plan(tree, np_, precision, tuning=cfg) for cfg in configs]
+                    ready.put((ci, ppb, pts, tree, base, plans, u))
+                ready.put((ci, None, None, None, None, None, 0.0))
+        except Exception as ex:  # reported by the timing loop
+            errors.append(ex)
+            ready.put(None)
+
+    pool = [threading.Thread(target=worker, daemon=True) for _ in range(threads)]
+    for t in pool:
+        t.start()
+    rows_f, rows_t, cloud, ppbs, cfgs = [], [], [], [], []
+    done = 0
+    while done < len(specs):
+        item = ready.get()
+        if item is None:
+            raise errors[0]
+        ci, ppb, pts, tree, base, plans, u = item
+        if ppb is None:
+            done += 1
+            if log:
+                log(f"cloud {ci} {specs[ci]['kind']} n={specs[ci]['n']}: done ({done}/{len(specs)})")
+            continue
+        for k, (cfg, plan) in enumerate(zip(configs, plans)):
+            rows_f.append(np.concatenate([base, config_features(cfg)]))
+            rows_t.append(time_phases(K, plan, pts))
             cloud.append(ci)
             ppbs.append(ppb)
-        if log:
-            log(f"cloud {ci} {sp['kind']} n={sp['n']}: done")
+            cfgs.append(k)
+            plan.close()
+        tree.close()
+        release(u)
+    for t in pool:
+        t.join()
     return {"features": np.array(rows_f), "phase_ms": np.array(rows_t), "cloud": np.array(cloud),
-            "ppb": np.array(ppbs), "n": np.array([specs[c]["n"] for c in cloud]),
+            "ppb": np.array(ppbs), "config": np.array(cfgs),
+            "n": np.array([specs[c]["n"] for c in cloud]),
             "kind": np.array([specs[c]["kind"] for c in cloud]),
             "seed": np.array([specs[c]["seed"] for c in cloud])}
 
@@ -244,36 +339,48 @@ class CostModel:
         z = np.load(path)
         return cls(K, z["mean"], z["std"], z["params"], int(z["hidden"]))
 
-    def pick(self, pts, np_=6, precision=None, leaf_sizes=LEAF_SIZES, fallback_margin=0.10):
-        """(leaf size, {leaf size: predicted ms}, measured?) for a cloud."""
+    def pick(self, pts, np_=6, precision=None, leaf_sizes=LEAF_SIZES, configs=CONFIGS,
+             fallback_margin=0.10):
+        """((leaf size, configuration), {(leaf size, config index): predicted
+        ms}, measured?) for a cloud."""
         K = self.K
         precision = K.MIXED if precision is None else precision
         n = len(pts["sx"])
         args = [pts[k] for k in ("sx", "sy", "sz", "tx", "ty", "tz")]
         cand = [b for b in leaf_sizes if b * 8 <= n] or [leaf_sizes[0]]
-        feats = []
+        keys, feats = [], []
         for ppb in cand:
             tree = K.Tree(*args, ppb, device=True)
-            feats.append(features(tree, np_, ppb, n))
+            base = tree_features(tree, np_, ppb, n)
             tree.close()
-        pred = dict(zip(cand, self.predict_ms(np.array(feats))))
-        order = sorted(cand, key=pred.get)
-        if len(order) > 1 and pred[order[1]] - pred[order[0]] < fallback_margin * pred[order[0]]:
+            for k, cfg in enumerate(configs):
+                keys.append((ppb, k))
+                feats.append(np.concatenate([base, config_features(cfg)]))
+        pred = dict(zip(keys, self.predict_ms(np.array(feats))))
+        order = sorted(keys, key=pred.get)
+        best = order[0]
+        measured = len(order) > 1 and pred[order[1]] - pred[order[0]] < fallback_margin * pred[order[0]]
+        if measured:
             from . import autotune
-            ms = {b: autotune.time_leaf_size(K, pts, b, np_, precision) for b in order[:2]}
-            return min(ms, key=ms.get), pred, True
-        return order[0], pred, False
+            ms = {key: autotune.time_leaf_size(K, pts, key[0], np_, precision,
+                                               tuning=configs[key[1]]) for key in order[:2]}
+            best = min(ms, key=ms.get)
+        return (best[0], dict(configs[best[1]])), pred, measured
 
 
 def evaluate_picks(model, data, clouds, default_ppb=512, fallback_margin=0.10):
     """For each cloud of the dataset, from the harvested measurements: the
-    time of the model's pick, of the model with the measured fallback (the
-    two best predictions measured when they are within fallback_margin), of
-    the fixed default and of the sweep's best.  Ratios to the best."""
+    time of the model's pick over all measured (leaf size, configuration)
+    rows, of the model with the measured fallback (the two best predictions
+    measured when they are within fallback_margin), of the fixed default
+    (leaf size 512 with the automatic configuration) and of the sweep's best.
+    Ratios to the best."""
     out = []
+    cfg_col = data["config"] if "config" in data else np.zeros(len(data["ppb"]), int)
     for c in clouds:
         m = data["cloud"] == c
         ppb = data["ppb"][m]
+        cfg = cfg_col[m]
         total = data["phase_ms"][m].sum(1)
         pred = model.predict_ms(data["features"][m])
         best = total.min()
@@ -283,12 +390,14 @@ def evaluate_picks(model, data, clouds, default_ppb=512, fallback_margin=0.10):
         measured = len(order) > 1 and pred[order[1]] - pred[order[0]] < fallback_margin * pred[order[0]]
         if measured:
             fb = order[:2][np.argmin(total[order[:2]])]
-        dflt = total[ppb == default_ppb][0] if np.any(ppb == default_ppb) else total[-1]
+        sel = (ppb == default_ppb) & (cfg == 0)
+        dflt = total[sel][0] if np.any(sel) else total[-1]
         out.append({"cloud": int(c), "kind": str(data["kind"][m][0]), "n": int(data["n"][m][0]),
                     "pick_over_best": float(total[pick] / best),
                     "fallback_over_best": float(total[fb] / best), "measured": bool(measured),
                     "default_over_best": float(dflt / best),
-                    "picked": int(ppb[pick]), "best": int(ppb[np.argmin(total)])})
+                    "picked": (int(ppb[pick]), int(cfg[pick])),
+                    "best": (int(ppb[np.argmin(total)]), int(cfg[np.argmin(total)]))})
     return out
 
 
@@ -298,7 +407,8 @@ def main(argv):
     K = __graft_entry__.load_package()
     if argv[0] == "harvest":
         specs = cloud_specs(int(argv[2]))
-        data = harvest(K, specs, log=print)
+        threads = int(argv[3]) if len(argv) > 3 else 8
+        data = harvest(K, specs, threads=threads, log=lambda m: print(m, flush=True))
         np.savez_compressed(argv[1], **data)
     elif argv[0] == "train":
         data = dict(np.load(argv[1]))
@@ -310,3 +420,8 @@ def main(argv):
         held = sorted(set(data["cloud"][~train].tolist()))
         ev = evaluate_picks(model, data, held)
         print(json.dumps({"final_loss": float(losses[-1]), "held_out": ev}))
+
+
+if __name__ == "__main__":
+    import sys
+    main(sys.argv[1:])

@@ -1,6 +1,7 @@
-"""Batched solves under one CUDA graph (kfmm_batch_*), with leaf sizes from
-the autotuner: a smaller instance of the batched workload (solves of uneven
-size, uniform cube and ellipsoid surface, NP 3 and 4, mixed form).
+"""Batched solves under one CUDA graph (kfmm_batch_*), with leaf sizes and
+launch choices from the autotuner: a smaller instance of the batched
+workload (solves of uneven size, uniform cube and ellipsoid surface, NP 3 and
+4, mixed form).
 
 * every solve's potentials from the graph replay equal, bit for bit, those of
   the same plan run on its own (the kernels are deterministic), on two
@@ -15,7 +16,9 @@ import pytest
 @pytest.mark.gpu
 def test_batched_graph_matches_single_runs(K, oracle_mod, cuda_ok, tmp_path):
     from kifmm_b200 import autotune, batched
-    table = autotune.LeafSizeTable(str(tmp_path / "leaf_sizes.json"))
+    table = autotune.ConfigTable(str(tmp_path / "configs.json"),
+                                 knobs=(("job_rows", (0, 4)), ("nf_blocks", (0, 5))),
+                                 candidates=(16, 32, 64))
     sp = batched.specs(12, nmin=4096, nmax=40000, seed=7)
     B = batched.BatchedSolves(K, sp, K.MIXED, table=table, nstreams=4, num_check=60)
     single = []
@@ -38,7 +41,8 @@ def test_batched_graph_matches_single_runs(K, oracle_mod, cuda_ok, tmp_path):
         print(f"{s['distribution']} n={s['n']} np={s['np']} ppb={s['ppb']}: mixed {e_mixed:.3e} "
               f"plain {e_plain:.3e}")
         assert e_mixed <= 2.0 * e_plain
-    assert (tmp_path / "leaf_sizes.json").exists()
+    assert (tmp_path / "configs.json").exists()
+    assert any(s["tuning"] is not None for s in B.solves)
     B.close()
 
 

@@ -54,7 +54,9 @@ def test_features_and_clusters(K):
         assert np.all(pts[k] >= -1) and np.all(pts[k] < 1)
     tree = K.Tree(*[pts[k] for k in ("sx", "sy", "sz", "tx", "ty", "tz")], 64)
     f = costmodel.features(tree, 6, 64, 20000)
-    assert f.shape == (3 + costmodel.NLEVELS + 5 * costmodel.NBINS + 12,)
+    assert f.shape == (3 + costmodel.NLEVELS + 5 * costmodel.NBINS + 12 + 2,)
+    g = costmodel.features(tree, 6, 64, 20000, costmodel.CONFIGS[1])
+    assert np.array_equal(f[:-2], g[:-2]) and not np.array_equal(f[-2:], g[-2:])
     assert np.all(np.isfinite(f))
 
 
