@@ -149,6 +149,11 @@ typedef struct {
 kfmm_status kfmm_plan_create_tuned(const kfmm_tree_desc* tree, int np, kfmm_precision precision,
                                    const kfmm_operator_set* ops, const kfmm_tuning* tuning,
                                    kfmm_plan** out);
+/* New launch choices for an existing plan (NULL: all automatic): the
+ * near-field jobs are re-chunked, the other choices are launch shapes; it
+ * waits for the device first.  A batch that holds the plan must be created
+ * again afterwards.  Only the split-K factor changes the order of any sum. */
+kfmm_status kfmm_plan_set_tuning(kfmm_plan* plan, const kfmm_tuning* tuning);
 kfmm_status kfmm_plan_destroy(kfmm_plan* plan);
 
 /* Points in ORIGINAL order.  Host variants copy host->device inside the call

@@ -80,6 +80,7 @@ def lib():
                                             ctypes.POINTER(OperatorSet), ctypes.POINTER(vp)],
         "kfmm_plan_create_tuned": [ctypes.POINTER(TreeDesc), i, i, ctypes.POINTER(OperatorSet),
                                    ctypes.POINTER(Tuning), ctypes.POINTER(vp)],
+        "kfmm_plan_set_tuning": [vp, ctypes.POINTER(Tuning)],
         "kfmm_plan_destroy": [vp],
         "kfmm_set_sources": [vp, _f64p, _f64p, _f64p, _f64p, vp],
         "kfmm_set_targets": [vp, _f64p, _f64p, _f64p, vp],
@@ -282,6 +283,11 @@ class Plan:
         s = Stats()
         check(lib().kfmm_plan_stats(self.handle, ctypes.byref(s)), "plan_stats")
         return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def set_tuning(self, tuning=None):
+        """New launch choices (dict of kfmm_tuning fields; None: automatic)."""
+        t = ctypes.byref(Tuning(**{k: int(v) for k, v in tuning.items()})) if tuning else None
+        check(lib().kfmm_plan_set_tuning(self.handle, t), "plan_set_tuning")
 
     def set_wait_limit(self, tries):
         """Tries of the kernels' bounded waits; < 0 restores the default."""

@@ -40,19 +40,26 @@ MIXED_ONLY = ("nf_blocks", "had_windows")
 KEEP_GAIN = 0.005
 
 
+def time_run(plan, reps=3):
+    """Device milliseconds of one kfmm_run of a plan whose points are set
+    (minimum over reps, after one warm-up run)."""
+    plan.run()
+    plan.enable_timing(True)
+    best = math.inf
+    for _ in range(reps):
+        plan.run()
+        best = min(best, sum(plan.kernel_times().values()))
+    plan.enable_timing(False)
+    return best
+
+
 def time_plan(K, tree, pts, np_, precision, tuning=None, reps=3):
-    """Device milliseconds of one kfmm_run (minimum over reps, after one
-    warm-up run) of a plan over `tree` with the given launch choices."""
+    """Device milliseconds of one kfmm_run of a plan over `tree` with the
+    given launch choices; the plan is built and released here."""
     plan = K.Plan(tree, np_, precision, tuning=tuning or None)
     try:
         plan.set_points(pts)
-        plan.run()
-        plan.enable_timing(True)
-        best = math.inf
-        for _ in range(reps):
-            plan.run()
-            best = min(best, sum(plan.kernel_times().values()))
-        return best
+        return time_run(plan, reps)
     finally:
         plan.close()
 
@@ -89,6 +96,8 @@ def tune(K, pts, np_, precision, candidates=CANDIDATES, knobs=KNOBS, reps=3):
     best, best_ms = {}, leaf_ms[ppb]
     sweep = {}
     tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], ppb)
+    plan = K.Plan(tree, np_, precision)  # one plan, its launch choices changed in place
+    plan.set_points(pts)
     try:
         for name, values in knobs:
             if name in MIXED_ONLY and precision != K.MIXED:
@@ -102,11 +111,13 @@ def tune(K, pts, np_, precision, candidates=CANDIDATES, knobs=KNOBS, reps=3):
                     cfg[name] = v
                 else:
                     cfg.pop(name, None)
-                ms = time_plan(K, tree, pts, np_, precision, cfg, reps)
+                plan.set_tuning(cfg)
+                ms = time_run(plan, reps)
                 sweep[name][v] = ms
                 if ms < best_ms * (1.0 - KEEP_GAIN):
                     best, best_ms = cfg, ms
     finally:
+        plan.close()
         tree.close()
     return {"ppb": ppb, "tuning": best, "ms": best_ms,
             "sweep": {"leaf": leaf_ms, "knobs": sweep}}

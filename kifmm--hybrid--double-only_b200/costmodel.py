@@ -167,10 +167,11 @@ def tree_features(tree, np_, ppb, n):
     return np.array(f, np.float64)
 
 
-def time_phases(K, plan, pts, reps=2):
+def time_phases(K, plan, pts, reps=2, set_points=True):
     """Per-phase device ms of one solve (minimum over reps after a warm-up),
     the copy phase counted into down."""
-    plan.set_points(pts)
+    if set_points:
+        plan.set_points(pts)
     plan.run()
     plan.enable_timing(True)
     best = None
@@ -192,13 +193,15 @@ def measure(K, pts, np_, ppb, precision, reps=2, device_tree=True, configs=CONFI
     try:
         base = tree_features(tree, np_, ppb, len(pts["sx"]))
         out = []
-        for cfg in configs:
-            plan = K.Plan(tree, np_, precision, tuning=cfg)
-            try:
+        plan = K.Plan(tree, np_, precision, tuning=configs[0])
+        try:
+            for k, cfg in enumerate(configs):
+                if k:
+                    plan.set_tuning(cfg)
                 out.append((np.concatenate([base, config_features(cfg)]),
-                            time_phases(K, plan, pts, reps)))
-            finally:
-                plan.close()
+                            time_phases(K, plan, pts, reps, set_points=(k == 0))))
+        finally:
+            plan.close()
         return out
     finally:
         tree.close()
@@ -253,12 +256,12 @@ def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, configs=CONF
                 for ppb in leaf_sizes:
                     if ppb * 8 > sp["n"]:
                         continue
-                    u = 600.0 * sp["n"] * len(configs)
+                    u = 600.0 * sp["n"]
                     reserve(u)
                     tree = K.Tree(*args, ppb)
                     base = tree_features(tree, np_, ppb, sp["n"])
-                    plans = [K.Plan(tree, np_, precision, tuning=cfg) for cfg in configs]
-                    ready.put((ci, ppb, pts, tree, base, plans, u))
+                    plan = K.Plan(tree, np_, precision, tuning=configs[0])
+                    ready.put((ci, ppb, pts, tree, base, plan, u))
                 ready.put((ci, None, None, None, None, None, 0.0))
         except Exception as ex:  # reported by the timing loop
             errors.append(ex)
@@ -273,19 +276,21 @@ def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, configs=CONF
         item = ready.get()
         if item is None:
             raise errors[0]
-        ci, ppb, pts, tree, base, plans, u = item
+        ci, ppb, pts, tree, base, plan, u = item
         if ppb is None:
             done += 1
             if log:
                 log(f"cloud {ci} {specs[ci]['kind']} n={specs[ci]['n']}: done ({done}/{len(specs)})")
             continue
-        for k, (cfg, plan) in enumerate(zip(configs, plans)):
+        for k, cfg in enumerate(configs):
+            if k:
+                plan.set_tuning(cfg)
             rows_f.append(np.concatenate([base, config_features(cfg)]))
-            rows_t.append(time_phases(K, plan, pts))
+            rows_t.append(time_phases(K, plan, pts, set_points=(k == 0)))
             cloud.append(ci)
             ppbs.append(ppb)
             cfgs.append(k)
-            plan.close()
+        plan.close()
         tree.close()
         release(u)
     for t in pool:

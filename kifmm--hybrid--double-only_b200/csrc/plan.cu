@@ -102,6 +102,11 @@ struct kfmm_plan {
   int *s2m_ent = nullptr, *nf_ent = nullptr, *s2l_ent = nullptr;
   int n_s2m = 0, n_nf = 0, n_s2l = 0;
   std::vector<float> nf_class;  // cost class of each near-field job (-log1.25 cost)
+  // the near field's jobs before chunking (one per target leaf, all its
+  // targets) and their source counts, kept to re-chunk on a new job size
+  std::vector<P2PJob> nf_leaf;
+  std::vector<double> nf_leaf_ns;
+  bool nf_w_heavy = false;     // W-list surfaces carry > 1% of the near-field pairs
   int* job_counter = nullptr;  // persistent P2P work counters: S2M, S2L, near field
   // [0] set by kernels whose bounded waits ran out, zeroed per solve; [1]
   // collects [0] over the kfmm_evaluate_async calls since the last wait
@@ -161,6 +166,15 @@ kfmm_status dalloc(kfmm_plan* p, T** ptr, size_t count) {
 }
 
 template <class T>
+void dfree(kfmm_plan* p, T*& ptr) {
+  if (!ptr) return;
+  auto it = std::find(p->allocs.begin(), p->allocs.end(), (void*)ptr);
+  if (it != p->allocs.end()) p->allocs.erase(it);
+  cudaFree(ptr);
+  ptr = nullptr;
+}
+
+template <class T>
 kfmm_status upload(kfmm_plan* p, T** ptr, const std::vector<T>& h) {
   kfmm_status s = dalloc(p, ptr, h.size());
   if (s != KFMM_OK) return s;
@@ -173,6 +187,49 @@ kfmm_status upload(kfmm_plan* p, T** ptr, const std::vector<T>& h) {
     kfmm_status s_ = (x);          \
     if (s_ != KFMM_OK) return s_;  \
   } while (0)
+
+// Split K when the launch would give fewer than two blocks per SM.  The split
+// count minimises (waves of blocks) x (16-deep K slices per block) plus the
+// split-K partial sums' traffic, 16 B per entry per split, counted at ~12.5 MB
+// per slice-wave (the kernel's measured rate): one wave of half-K blocks
+// beats two waves of third-K blocks.  At most kSplitKAuto ways unless the
+// plan's tuning says otherwise: the autotuner found 4 ways faster than the
+// model's own optimum (up to K / 64 ways) on small and mid-size trees, where
+// the extra split's partial sums and reduction launch cost more than the
+// model counts.
+constexpr int kSplitKAuto = 4;
+void choose_split(const kfmm_plan* p, GemmBatch& g) {
+  const int M = g.M, K = g.K;
+  const int blocks = g.chunks * ((g.ncol + kGemmBN - 1) / kGemmBN);
+  const int want = 2 * p->num_sms;
+  g.nsplit = 1;
+  g.ksplit = (K + kGemmBK - 1) / kGemmBK * kGemmBK;
+  if (blocks >= want) return;
+  double best = 1e300;
+  const int smax = p->tune.splitk_max > 0 ? p->tune.splitk_max
+                                          : std::min(kSplitKAuto, std::max(1, K / 64));
+  for (int s = 1; s <= smax; ++s) {
+    const int ks = ((K + s - 1) / s + kGemmBK - 1) / kGemmBK * kGemmBK;
+    const int ns = (K + ks - 1) / ks;
+    const double waves = std::ceil((double)blocks * ns / want);
+    const double traffic = ns > 1 ? ns * 16.0 * M * (double)g.ncol / 12.5e6 : 0.0;
+    const double cost = waves * (ks / kGemmBK) + traffic;
+    if (cost < best) {
+      best = cost;
+      g.nsplit = ns;
+      g.ksplit = ks;
+    }
+  }
+}
+
+// Split-K scratch the plan's level products need (doubles).
+size_t splitk_need(const kfmm_plan* p) {
+  size_t n = 0;
+  for (const auto* v : {&p->up_gemms, &p->down_gemms})
+    for (const GemmBatch& g : *v)
+      if (g.nsplit > 1) n = std::max(n, (size_t)g.nsplit * g.ncol * g.M);
+  return n;
+}
 
 kfmm_status add_gemm(kfmm_plan* p, std::vector<GemmBatch>& out, const double* A, int M, int K,
                      const double* B, const std::vector<int>& boff, double* C,
@@ -198,36 +255,9 @@ kfmm_status add_gemm(kfmm_plan* p, std::vector<GemmBatch>& out, const double* A,
   KF_TRY(upload(p, &g.boff, boff));
   KF_TRY(upload(p, &g.coff, coff));
   if (alpha) KF_TRY(upload(p, &g.alpha, *alpha));
-  // rows in near-equal chunks of <= kGemmRows (multiples of 8); split K when
-  // the launch would give fewer than two blocks per SM.  The split count
-  // minimises (waves of blocks) x (16-deep K slices per block) plus the
-  // split-K partial sums' traffic, 16 B per entry per split, counted at
-  // ~12.5 MB per slice-wave (the kernel's measured rate): one wave of half-K
-  // blocks beats two waves of third-K blocks.
   g.chunks = (M + kGemmRows - 1) / kGemmRows;
   g.mrows = ((M + g.chunks - 1) / g.chunks + 7) / 8 * 8;
-  const int blocks = g.chunks * ((g.ncol + kGemmBN - 1) / kGemmBN);
-  const int want = 2 * p->num_sms;
-  g.nsplit = 1;
-  g.ksplit = (K + kGemmBK - 1) / kGemmBK * kGemmBK;
-  if (blocks < want) {
-    double best = 1e300;
-    const int smax = p->tune.splitk_max > 0 ? p->tune.splitk_max : std::max(1, K / 64);
-    for (int s = 1; s <= smax; ++s) {
-      const int ks = ((K + s - 1) / s + kGemmBK - 1) / kGemmBK * kGemmBK;
-      const int ns = (K + ks - 1) / ks;
-      const double waves = std::ceil((double)blocks * ns / want);
-      const double traffic = ns > 1 ? ns * 16.0 * M * (double)g.ncol / 12.5e6 : 0.0;
-      const double cost = waves * (ks / kGemmBK) + traffic;
-      if (cost < best) {
-        best = cost;
-        g.nsplit = ns;
-        g.ksplit = ks;
-      }
-    }
-  }
-  if (g.nsplit > 1)
-    p->splitk_doubles = std::max(p->splitk_doubles, (size_t)g.nsplit * g.ncol * M);
+  choose_split(p, g);
   p->stats.gemm_flops += 2.0 * M * (double)K * g.ncol;
   out.push_back(g);
   return KFMM_OK;
@@ -366,6 +396,91 @@ kfmm_status validate_desc(const kfmm_tree_desc* d) {
 // Key of a position within one level (coordinates < 2^21: plans accept depth <= 21).
 inline long long key_of(int x, int y, int z) {
   return (long long)x | ((long long)y << 21) | ((long long)z << 42);
+}
+
+// The near field's jobs: each target leaf's targets in chunks of 32 * rows
+// (rows: the tuning's job_rows, else 4 for mixed plans whose W-list surfaces
+// carry more than 1% of the pairs, else 6), ordered largest first by cost
+// class (target slots x sources, in classes 25% wide); within a class the
+// jobs keep their tree order, so warps working at the same time read
+// neighbouring leaves' sources and the L2 cache serves the repeats.  The
+// mixed near field runs with 5 resident blocks per SM on the same clouds
+// (or when the tuning says so).  Measured on 4M points on the ellipsoid
+// surface, NP=4, 256 per box: 2.32 ms against 2.50 ms with 6 blocks and 6
+// rows; uniform clouds keep 6 and 6 (4.42 ms, against 4.70 ms with 4 rows).
+kfmm_status build_nf_jobs(kfmm_plan* p) {
+  int rows = p->prec == KFMM_MIXED && p->nf_w_heavy ? 4 : kMaxSlots;
+  if (p->tune.job_rows > 0) rows = std::min(p->tune.job_rows, kMaxSlots);
+  const int chunk = 32 * rows;
+  std::vector<P2PJob> jobs;
+  std::vector<double> ns;
+  for (size_t l = 0; l < p->nf_leaf.size(); ++l) {
+    const P2PJob& L = p->nf_leaf[l];
+    for (int c = 0; c < L.tcnt; c += chunk) {
+      P2PJob j = L;
+      j.tbeg = L.tbeg + c;
+      j.tcnt = std::min(chunk, L.tcnt - c);
+      j.out = L.out + c;
+      jobs.push_back(j);
+      ns.push_back(p->nf_leaf_ns[l]);
+    }
+  }
+  std::vector<std::pair<double, int>> key(jobs.size());
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    const double cost = std::max(1.0, ns[j] * ((jobs[j].tcnt + 31) / 32));
+    key[j] = {-std::floor(std::log(cost) / std::log(1.25)), (int)j};
+  }
+  std::stable_sort(key.begin(), key.end(),
+                   [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+                     return a.first < b.first;
+                   });
+  std::vector<P2PJob> out(jobs.size());
+  p->nf_class.resize(jobs.size());
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    out[j] = jobs[key[j].second];
+    p->nf_class[j] = (float)key[j].first;
+  }
+  dfree(p, p->nf_jobs);
+  KF_TRY(upload(p, &p->nf_jobs, out));
+  p->n_nf = (int)out.size();
+  p->nf_minb5 = p->prec == KFMM_MIXED &&
+                (p->tune.nf_blocks == 5 || (p->tune.nf_blocks == 0 && p->nf_w_heavy));
+  return KFMM_OK;
+}
+
+// Mixed Hadamard launch shape: one CTA per SM over (chunks x frequency
+// blocks).  A chunk holds k windows per warp (every warp the same count, so
+// none idles at the end of its CTA); k minimises the span ceil(CTAs / SMs) x
+// (k + 0.1), the 0.1 standing for a CTA's translation-tile load, unless the
+// tuning fixes k.
+void set_had_blocks(kfmm_plan* p) {
+  const int nfb = p->Fpad / kFB;
+  auto per_block = [&](int items, int warps) {
+    if (p->tune.had_windows > 0) return warps * std::min(p->tune.had_windows, 8);
+    int pick = warps;
+    double best = 1e300;
+    for (int k = 1; k <= 8; ++k) {
+      const long long ctas = (long long)((items + warps * k - 1) / (warps * k)) * nfb;
+      const double span = std::ceil((double)ctas / p->num_sms) * (k + 0.1);
+      if (span < best) {
+        best = span;
+        pick = warps * k;
+      }
+    }
+    return pick;
+  };
+  p->had32_groups_per_block = per_block(p->n_singles, kHad32Warps);
+  p->pair_per_block = per_block(p->n_pairs, kHadPairWarps);
+}
+
+kfmm_status check_tuning(const kfmm_tuning* t) {
+  if (t && (t->nf_blocks < 0 || t->nf_blocks > 6 || (t->nf_blocks > 0 && t->nf_blocks < 5) ||
+            t->job_rows < 0 || t->job_rows > kMaxSlots || t->had_windows < 0 ||
+            t->had_windows > 8 || t->splitk_max < 0)) {
+    set_error("kfmm_tuning: tuning value out of range");
+    return KFMM_ERR_INVALID;
+  }
+  return KFMM_OK;
 }
 
 kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operator_set* user) {
@@ -537,7 +652,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_CUDA(cudaMemset(p->spec, 0, p->cplx * (size_t)nn * p->Fpad));
   KF_CUDA(cudaMemset(p->effv, 0, p->cplx * (size_t)nn * p->Fpad));
 
-  int chunk = 32 * kMaxSlots;  // targets per job (the near field's is chosen below)
+  const int chunk = 32 * kMaxSlots;  // targets per S2M / S2L job (near field: build_nf_jobs)
   auto add_chunks = [&](std::vector<P2PJob>& jobs, int tnode, int tkind, int tbeg0, int tcount,
                         int ebeg, int eend, int out0, int mode) {
     for (int c = 0; c < tcount; c += chunk) {
@@ -830,10 +945,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       for (int k = d->u_ptr[t]; k < d->u_ptr[t + 1]; ++k) ns += d->src_num[d->u_idx[k]];
       all_pairs += ns * d->trg_num[t];
     }
-    const bool w_heavy = w_pairs > 0.01 * (all_pairs + w_pairs);
-    int rows = p->prec == KFMM_MIXED && w_heavy ? 4 : kMaxSlots;
-    if (p->tune.job_rows > 0) rows = std::min(p->tune.job_rows, kMaxSlots);
-    chunk = 32 * rows;
+    p->nf_w_heavy = w_pairs > 0.01 * (all_pairs + w_pairs);
     for (int t = 0; t < nn; ++t) {
       if (!is_leaf(t) || !has_trg(t) || d->trg_num[t] == 0) continue;
       int e0 = (int)ent.size();
@@ -848,15 +960,21 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       if (d->depth[t] >= 2) ent.push_back((2 << 28) | t);
       int ns = 0;
       for (int k = e0; k < (int)ent.size(); ++k) ns += src_count(ent[k]);
-      add_chunks(jobs, t, 0, d->trg_beg[t], d->trg_num[t], e0, (int)ent.size(), d->trg_beg[t], 0);
+      P2PJob j;
+      j.tnode = t;
+      j.tkind = 0;
+      j.tbeg = d->trg_beg[t];
+      j.tcnt = d->trg_num[t];
+      j.ebeg = e0;
+      j.eend = (int)ent.size();
+      j.out = d->trg_beg[t];
+      j.mode = 0;
+      p->nf_leaf.push_back(j);
+      p->nf_leaf_ns.push_back(ns);
       p->stats.u_pairs += (double)d->trg_num[t] * ns;
     }
-    order_jobs(jobs, ent, &p->nf_class);
-    p->n_nf = (int)jobs.size();
-    p->nf_minb5 = p->prec == KFMM_MIXED && (p->tune.nf_blocks == 5 ||
-                                            (p->tune.nf_blocks == 0 && w_heavy));
-    KF_TRY(upload(p, &p->nf_jobs, jobs));
     KF_TRY(upload(p, &p->nf_ent, ent));
+    KF_TRY(build_nf_jobs(p));
   }
 
   KF_CUDA(cudaFuncSetAttribute(gemm_fp64_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -866,30 +984,9 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_CUDA(cudaFuncSetAttribute(hadamard_fp32_pair_kernel,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kHadPairSmemBytes));
-  {
-    // One CTA per SM over (chunks x frequency blocks).  A chunk holds k
-    // windows per warp (every warp the same count, so none idles at the end
-    // of its CTA); k minimises the span ceil(CTAs / SMs) x (k + 0.1), the 0.1
-    // standing for a CTA's translation-tile load.
-    const int nfb = p->Fpad / kFB;
-    auto per_block = [&](int items, int warps) {
-      if (p->tune.had_windows > 0) return warps * std::min(p->tune.had_windows, 8);
-      int pick = warps;
-      double best = 1e300;
-      for (int k = 1; k <= 8; ++k) {
-        const long long ctas = (long long)((items + warps * k - 1) / (warps * k)) * nfb;
-        const double span = std::ceil((double)ctas / p->num_sms) * (k + 0.1);
-        if (span < best) {
-          best = span;
-          pick = warps * k;
-        }
-      }
-      return pick;
-    };
-    p->had32_groups_per_block = per_block(p->n_singles, kHad32Warps);
-    p->pair_per_block = per_block(p->n_pairs, kHadPairWarps);
-  }
+  set_had_blocks(p);
 
+  p->splitk_doubles = splitk_need(p);
   if (p->splitk_doubles) KF_TRY(dalloc(p, &p->splitk, p->splitk_doubles));
   KF_TRY(dalloc(p, &p->job_counter, 3));
   KF_TRY(dalloc(p, &p->d_error, 2));
@@ -903,12 +1000,10 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       KF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p2p_warp_kernel<false>,
                                                             32 * kWarpJobsPerBlock, 0));
     p->p2p_grid = std::max(1, occ) * p->num_sms;
-    if (p->nf_minb5) {
-      int occ5 = 0;
-      KF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, p2p_warp_kernel<true, 5>,
-                                                            32 * kWarpJobsPerBlock, 0));
-      p->p2p_grid5 = std::max(1, occ5) * p->num_sms;
-    }
+    int occ5 = 0;
+    KF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ5, p2p_warp_kernel<true, 5>,
+                                                          32 * kWarpJobsPerBlock, 0));
+    p->p2p_grid5 = std::max(1, occ5) * p->num_sms;
   }
   p->stats.num_nodes = nn;
   p->stats.P = P;
@@ -1033,13 +1128,7 @@ kfmm_status kfmm_plan_create_tuned(const kfmm_tree_desc* tree, int np, kfmm_prec
     return KFMM_ERR_INVALID;
   }
   KF_TRY(validate_desc(tree));
-  if (tuning && (tuning->nf_blocks < 0 || tuning->nf_blocks > 6 ||
-                 (tuning->nf_blocks > 0 && tuning->nf_blocks < 5) || tuning->job_rows < 0 ||
-                 tuning->job_rows > kMaxSlots || tuning->had_windows < 0 ||
-                 tuning->had_windows > 8 || tuning->splitk_max < 0)) {
-    set_error("kfmm_plan_create_tuned: tuning value out of range");
-    return KFMM_ERR_INVALID;
-  }
+  KF_TRY(check_tuning(tuning));
   kfmm_plan* p = new kfmm_plan();
   p->np = np;
   p->prec = precision;
@@ -1065,6 +1154,31 @@ kfmm_status kfmm_plan_destroy(kfmm_plan* p) {
   if (p->side) cudaStreamDestroy(p->side);
   if (p->d2h) cudaStreamDestroy(p->d2h);
   delete p;
+  return KFMM_OK;
+}
+
+kfmm_status kfmm_plan_set_tuning(kfmm_plan* p, const kfmm_tuning* tuning) {
+  if (!p) {
+    set_error("kfmm_plan_set_tuning: null plan");
+    return KFMM_ERR_INVALID;
+  }
+  KF_TRY(check_tuning(tuning));
+  const kfmm_tuning old = p->tune;
+  p->tune = tuning ? *tuning : kfmm_tuning{};
+  KF_CUDA(cudaDeviceSynchronize());  // no launch of the plan may still read what changes
+  if (p->tune.job_rows != old.job_rows || p->tune.nf_blocks != old.nf_blocks)
+    KF_TRY(build_nf_jobs(p));
+  set_had_blocks(p);
+  if (p->tune.splitk_max != old.splitk_max) {
+    for (auto* v : {&p->up_gemms, &p->down_gemms})
+      for (GemmBatch& g : *v) choose_split(p, g);
+    const size_t need = splitk_need(p);
+    if (need > p->splitk_doubles) {
+      dfree(p, p->splitk);
+      KF_TRY(dalloc(p, &p->splitk, need));
+      p->splitk_doubles = need;
+    }
+  }
   return KFMM_OK;
 }
 

@@ -54,3 +54,22 @@ def test_plan_rejects_bad_tuning(K):
     for bad in ({"nf_blocks": 3}, {"job_rows": 7}, {"had_windows": 9}, {"splitk_max": -1}):
         with pytest.raises(K.KfmmError, match="tuning value out of range"):
             K.Plan(tree, 4, K.MIXED, tuning=bad)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["plain", "mixed"])
+def test_set_tuning_in_place(K, cuda_ok, precision):
+    """Re-chunked near-field jobs, other resident-block counts and Hadamard
+    shapes give the same potentials bit for bit; a different split-K factor
+    reorders the level products' sums only (FP64 rounding)."""
+    prec = K.PLAIN_FP64 if precision == "plain" else K.MIXED
+    pts = K.generate_points(50000, "uniform", 0, 9)
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], 64)
+    want = K.Plan(tree, 6, prec).evaluate(pts)
+    plan = K.Plan(tree, 6, prec)
+    for cfg in ({"job_rows": 3}, {"job_rows": 1, "nf_blocks": 5, "had_windows": 2}, None):
+        plan.set_tuning(cfg)
+        assert np.array_equal(plan.evaluate(pts), want), cfg
+    plan.set_tuning({"splitk_max": 1})
+    got = plan.evaluate(pts)
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-9
