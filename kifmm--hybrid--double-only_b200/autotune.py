@@ -35,7 +35,7 @@ CANDIDATES = (16, 32, 64, 128, 256, 512, 1024)
 KNOBS = (("job_rows", (0, 3, 4, 5, 6)),
          ("nf_blocks", (0, 5, 6)),
          ("had_windows", (0, 2, 4, 6, 8)),
-         ("splitk_max", (0, 1, 2, 4)))
+         ("splitk_max", (0, 1, 2, 4, 16)))
 MIXED_ONLY = ("nf_blocks", "had_windows")
 KEEP_GAIN = 0.005
 

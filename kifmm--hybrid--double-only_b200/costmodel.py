@@ -167,16 +167,18 @@ def tree_features(tree, np_, ppb, n):
     return np.array(f, np.float64)
 
 
-def time_phases(K, plan, pts, reps=2, set_points=True):
+def time_phases(K, plan, pts, reps=3, set_points=True, stream=None):
     """Per-phase device ms of one solve (minimum over reps after a warm-up),
-    the copy phase counted into down."""
+    the copy phase counted into down.  `stream`: a non-blocking stream keeps
+    other threads' synchronous copies (legacy stream) out of the timed
+    region."""
     if set_points:
-        plan.set_points(pts)
-    plan.run()
+        plan.set_points(pts, stream)
+    plan.run(stream)
     plan.enable_timing(True)
     best = None
     for _ in range(reps):
-        plan.run()
+        plan.run(stream)
         ph = plan.phase_times()
         v = np.array([ph[p] for p in PHASES])
         v[PHASES.index("down")] += ph["copy"]
@@ -218,13 +220,18 @@ def cloud_specs(count, nmin=65536, nmax=8388608, seed=5):
 
 
 def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, configs=CONFIGS,
-            threads=8, device_bytes=80e9, log=None):
+            threads=8, device_bytes=80e9, log=None, checkpoint=None):
     """Measured dataset: one row per (cloud, leaf size, configuration).
     `threads` workers build host trees, features and plans ahead of the
-    timing loop; at most `device_bytes` of plans (estimated at 600 bytes a
-    point each) are held at once."""
+    timing loop, which runs on its own non-blocking stream; at most
+    `device_bytes` of plans (estimated at 600 bytes a point each) are held at
+    once.  checkpoint(data): called with the rows so far every 100 clouds."""
     import queue
     import threading
+
+    import torch
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
     precision = K.MIXED if precision is None else precision
     ready = queue.Queue()
     held = [0.0]  # estimated device bytes of the plans built and not yet timed
@@ -272,6 +279,13 @@ def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, configs=CONF
         t.start()
     rows_f, rows_t, cloud, ppbs, cfgs = [], [], [], [], []
     done = 0
+
+    def pack():
+        return {"features": np.array(rows_f), "phase_ms": np.array(rows_t),
+                "cloud": np.array(cloud), "ppb": np.array(ppbs), "config": np.array(cfgs),
+                "n": np.array([specs[c]["n"] for c in cloud]),
+                "kind": np.array([specs[c]["kind"] for c in cloud]),
+                "seed": np.array([specs[c]["seed"] for c in cloud])}
     while done < len(specs):
         item = ready.get()
         if item is None:
@@ -281,12 +295,14 @@ def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, configs=CONF
             done += 1
             if log:
                 log(f"cloud {ci} {specs[ci]['kind']} n={specs[ci]['n']}: done ({done}/{len(specs)})")
+            if checkpoint and done % 100 == 0:
+                checkpoint(pack())
             continue
         for k, cfg in enumerate(configs):
             if k:
                 plan.set_tuning(cfg)
             rows_f.append(np.concatenate([base, config_features(cfg)]))
-            rows_t.append(time_phases(K, plan, pts, set_points=(k == 0)))
+            rows_t.append(time_phases(K, plan, pts, set_points=(k == 0), stream=sh))
             cloud.append(ci)
             ppbs.append(ppb)
             cfgs.append(k)
@@ -295,11 +311,7 @@ def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, configs=CONF
         release(u)
     for t in pool:
         t.join()
-    return {"features": np.array(rows_f), "phase_ms": np.array(rows_t), "cloud": np.array(cloud),
-            "ppb": np.array(ppbs), "config": np.array(cfgs),
-            "n": np.array([specs[c]["n"] for c in cloud]),
-            "kind": np.array([specs[c]["kind"] for c in cloud]),
-            "seed": np.array([specs[c]["seed"] for c in cloud])}
+    return pack()
 
 
 class CostModel:
@@ -413,7 +425,8 @@ def main(argv):
     if argv[0] == "harvest":
         specs = cloud_specs(int(argv[2]))
         threads = int(argv[3]) if len(argv) > 3 else 8
-        data = harvest(K, specs, threads=threads, log=lambda m: print(m, flush=True))
+        data = harvest(K, specs, threads=threads, log=lambda m: print(m, flush=True),
+                       checkpoint=lambda d: np.savez_compressed(argv[1], **d))
         np.savez_compressed(argv[1], **data)
     elif argv[0] == "train":
         data = dict(np.load(argv[1]))

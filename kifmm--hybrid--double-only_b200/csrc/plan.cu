@@ -192,12 +192,11 @@ kfmm_status upload(kfmm_plan* p, T** ptr, const std::vector<T>& h) {
 // count minimises (waves of blocks) x (16-deep K slices per block) plus the
 // split-K partial sums' traffic, 16 B per entry per split, counted at ~12.5 MB
 // per slice-wave (the kernel's measured rate): one wave of half-K blocks
-// beats two waves of third-K blocks.  At most kSplitKAuto ways unless the
-// plan's tuning says otherwise: the autotuner found 4 ways faster than the
-// model's own optimum (up to K / 64 ways) on small and mid-size trees, where
-// the extra split's partial sums and reduction launch cost more than the
-// model counts.
-constexpr int kSplitKAuto = 4;
+// beats two waves of third-K blocks.  Up to max(8, K / 64) ways unless the
+// plan's tuning says otherwise (measured on 4M points: allowing 8 ways to the
+// short-K products, K = P or Q, took 0.25 ms off the ellipsoid-surface solve
+// at NP=4 and 0.05 ms off the uniform one at NP=6, against K / 64 ways).
+constexpr int kSplitKAuto = 8;
 void choose_split(const kfmm_plan* p, GemmBatch& g) {
   const int M = g.M, K = g.K;
   const int blocks = g.chunks * ((g.ncol + kGemmBN - 1) / kGemmBN);
@@ -206,8 +205,7 @@ void choose_split(const kfmm_plan* p, GemmBatch& g) {
   g.ksplit = (K + kGemmBK - 1) / kGemmBK * kGemmBK;
   if (blocks >= want) return;
   double best = 1e300;
-  const int smax = p->tune.splitk_max > 0 ? p->tune.splitk_max
-                                          : std::min(kSplitKAuto, std::max(1, K / 64));
+  const int smax = p->tune.splitk_max > 0 ? p->tune.splitk_max : std::max(kSplitKAuto, K / 64);
   for (int s = 1; s <= smax; ++s) {
     const int ks = ((K + s - 1) / s + kGemmBK - 1) / kGemmBK * kGemmBK;
     const int ns = (K + ks - 1) / ks;

@@ -61,7 +61,9 @@ def test_plan_rejects_bad_tuning(K):
 def test_set_tuning_in_place(K, cuda_ok, precision):
     """Re-chunked near-field jobs, other resident-block counts and Hadamard
     shapes give the same potentials bit for bit; a different split-K factor
-    reorders the level products' sums only (FP64 rounding)."""
+    reorders the level products' sums only: FP64 rounding, amplified by the
+    pseudo-inverses' condition number, which the mixed form's FP32 rounding
+    of spectra and sources then shows at its own level (~1e-7)."""
     prec = K.PLAIN_FP64 if precision == "plain" else K.MIXED
     pts = K.generate_points(50000, "uniform", 0, 9)
     tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], 64)
@@ -72,4 +74,5 @@ def test_set_tuning_in_place(K, cuda_ok, precision):
         assert np.array_equal(plan.evaluate(pts), want), cfg
     plan.set_tuning({"splitk_max": 1})
     got = plan.evaluate(pts)
-    assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-9
+    tol = 1e-9 if precision == "plain" else 1e-6
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) < tol
