@@ -219,13 +219,28 @@ def cloud_specs(count, nmin=65536, nmax=8388608, seed=5):
     return out
 
 
+def plan_bytes(tree, np_, mixed=True):
+    """Upper estimate of a plan's device memory: per node the FP64 expansions
+    (3 x P), the leaf check potentials (Q) and two spectra (2 x (F padded to
+    32) complex, FP32 in the mixed form), per point the coordinates in both
+    orders, densities and potentials; 30% margin."""
+    P = np_ ** 3 - (np_ - 2) ** 3
+    Q = (np_ + 2) ** 3 - np_ ** 3
+    F = (np_ + 1) * (2 * np_) ** 2
+    fpad = (F + 31) // 32 * 32
+    d = tree.desc
+    per_node = 8.0 * (3 * P + Q) + 2 * (8.0 if mixed else 16.0) * fpad
+    per_point = 8.0 * 16 + 16.0
+    return 1.3 * (d.num_nodes * per_node + (d.num_src + d.num_trg) * per_point)
+
+
 def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, configs=CONFIGS,
-            threads=8, device_bytes=80e9, log=None, checkpoint=None):
+            threads=8, device_bytes=100e9, log=None, checkpoint=None):
     """Measured dataset: one row per (cloud, leaf size, configuration).
     `threads` workers build host trees, features and plans ahead of the
     timing loop, which runs on its own non-blocking stream; at most
-    `device_bytes` of plans (estimated at 600 bytes a point each) are held at
-    once.  checkpoint(data): called with the rows so far every 100 clouds."""
+    `device_bytes` of plans (plan_bytes) are held at once.
+    checkpoint(data): called with the rows so far every 100 clouds."""
     import queue
     import threading
 
@@ -263,9 +278,9 @@ def harvest(K, specs, np_=6, precision=None, leaf_sizes=LEAF_SIZES, configs=CONF
                 for ppb in leaf_sizes:
                     if ppb * 8 > sp["n"]:
                         continue
-                    u = 600.0 * sp["n"]
-                    reserve(u)
                     tree = K.Tree(*args, ppb)
+                    u = plan_bytes(tree, np_, precision == K.MIXED)
+                    reserve(u)
                     base = tree_features(tree, np_, ppb, sp["n"])
                     plan = K.Plan(tree, np_, precision, tuning=configs[0])
                     ready.put((ci, ppb, pts, tree, base, plan, u))
