@@ -75,6 +75,7 @@ struct kfmm_plan {
   double4* ctr = nullptr;
   int *d_depth = nullptr, *d_src_beg = nullptr, *d_src_num = nullptr;
   int *d_src_perm = nullptr, *d_trg_perm = nullptr;
+  int *d_src_inv = nullptr, *d_trg_inv = nullptr;  // original index -> leaf-order position
   // points
   double *o_sx = nullptr, *o_sy = nullptr, *o_sz = nullptr, *o_w = nullptr;
   double *o_tx = nullptr, *o_ty = nullptr, *o_tz = nullptr;
@@ -397,16 +398,21 @@ kfmm_status validate_desc(const kfmm_tree_desc* d) {
         return KFMM_ERR_INVALID;
       }
   }
-  for (int i = 0; i < d->num_src; ++i)
-    if (d->src_perm[i] < 0 || d->src_perm[i] >= d->num_src) {
-      set_error("kfmm_plan_create: source permutation out of range");
-      return KFMM_ERR_INVALID;
+  // permutations: every original index exactly once (the point reorders
+  // scatter through their inverses)
+  for (int pass = 0; pass < 2; ++pass) {
+    const int n = pass ? d->num_trg : d->num_src;
+    const int* perm = pass ? d->trg_perm : d->src_perm;
+    std::vector<char> seen(n, 0);
+    for (int i = 0; i < n; ++i) {
+      if (perm[i] < 0 || perm[i] >= n || seen[perm[i]]) {
+        set_error(pass ? "kfmm_plan_create: target permutation is not a permutation"
+                       : "kfmm_plan_create: source permutation is not a permutation");
+        return KFMM_ERR_INVALID;
+      }
+      seen[perm[i]] = 1;
     }
-  for (int i = 0; i < d->num_trg; ++i)
-    if (d->trg_perm[i] < 0 || d->trg_perm[i] >= d->num_trg) {
-      set_error("kfmm_plan_create: target permutation out of range");
-      return KFMM_ERR_INVALID;
-    }
+  }
   return KFMM_OK;
 }
 
@@ -567,6 +573,13 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_TRY(upload(p, &p->d_src_num, std::vector<int>(d->src_num, d->src_num + nn)));
   KF_TRY(upload(p, &p->d_src_perm, std::vector<int>(d->src_perm, d->src_perm + d->num_src)));
   KF_TRY(upload(p, &p->d_trg_perm, std::vector<int>(d->trg_perm, d->trg_perm + d->num_trg)));
+  {
+    std::vector<int> si(d->num_src), ti(d->num_trg);
+    for (int i = 0; i < d->num_src; ++i) si[d->src_perm[i]] = i;
+    for (int i = 0; i < d->num_trg; ++i) ti[d->trg_perm[i]] = i;
+    KF_TRY(upload(p, &p->d_src_inv, si));
+    KF_TRY(upload(p, &p->d_trg_inv, ti));
+  }
 
   // --- operators and surfaces
   KF_TRY(upload(p, &p->d_uc2ue, op.uc2ue));
@@ -1197,11 +1210,11 @@ kfmm_status kfmm_set_sources_device(kfmm_plan* p, const double* sx, const double
     return KFMM_ERR_INVALID;
   }
   if (p->prec == KFMM_MIXED) {
-    gather_sources_mixed_kernel<<<592, 256, 0, S(stream)>>>(p->ns, p->d_src_perm, p->d_src_leaf,
-                                                            sx, sy, sz, den, p->ctr, p->src4,
-                                                            p->src4f);
+    scatter_sources_mixed_kernel<<<4 * p->num_sms, 256, 0, S(stream)>>>(
+        p->ns, p->d_src_inv, p->d_src_leaf, sx, sy, sz, den, p->ctr, p->src4, p->src4f);
   } else {
-    gather_points_kernel<<<592, 256, 0, S(stream)>>>(p->ns, p->d_src_perm, sx, sy, sz, den, p->src4);
+    scatter_points_kernel<<<4 * p->num_sms, 256, 0, S(stream)>>>(p->ns, p->d_src_inv, sx, sy, sz,
+                                                                 den, p->src4);
   }
   KF_CHECK_LAUNCH("source gather");
   p->have_src = true;
@@ -1214,8 +1227,9 @@ kfmm_status kfmm_set_targets_device(kfmm_plan* p, const double* tx, const double
     set_error("kfmm_set_targets_device: null argument");
     return KFMM_ERR_INVALID;
   }
-  gather_points_kernel<<<592, 256, 0, S(stream)>>>(p->nt, p->d_trg_perm, tx, ty, tz, nullptr, p->trg4);
-  KF_CHECK_LAUNCH("gather_points_kernel");
+  scatter_points_kernel<<<4 * p->num_sms, 256, 0, S(stream)>>>(p->nt, p->d_trg_inv, tx, ty, tz,
+                                                               nullptr, p->trg4);
+  KF_CHECK_LAUNCH("scatter_points_kernel");
   p->have_trg = true;
   return KFMM_OK;
 }

@@ -75,6 +75,14 @@ def test_plan_create_argument_errors(K):
     bad.u_idx = u.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
     assert L.kfmm_plan_create(ctypes.byref(bad), 6, 0, ctypes.byref(h)) == 1
     assert b"out of range" in L.kfmm_last_error()
+    # a repeated index in the leaf-order permutation (points reach leaf order
+    # through its inverse)
+    bad = K.TreeDesc.from_buffer_copy(t.desc)
+    perm = t.array("src_perm").astype(np.int32)
+    perm[1] = perm[0]
+    bad.src_perm = perm.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    assert L.kfmm_plan_create(ctypes.byref(bad), 6, 0, ctypes.byref(h)) == 1
+    assert b"not a permutation" in L.kfmm_last_error()
 
 
 def test_plan_create_without_device_reports_status(K):
