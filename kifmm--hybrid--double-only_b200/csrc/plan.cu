@@ -134,8 +134,6 @@ struct kfmm_plan {
   int num_sms = 148;
   double* splitk = nullptr;   // split-K partial sums, shared by the level GEMMs
   size_t splitk_doubles = 0;
-  int* gemm_tiles = nullptr;  // split-K arrival counters per output tile (zero between launches)
-  size_t gemm_tiles_n = 0;
   bool timing = false;
   // timing marks (kfmm_enable_timing): 0 start, 1 S2M pairs done, 2 up done,
   // 3 forward FFT, 4 Hadamard, 5 inverse FFT (V done), 6 S2L (X done),
@@ -223,36 +221,37 @@ void choose_split(const kfmm_plan* p, GemmBatch& g) {
   }
 }
 
-// Split-K scratch the plan's level products need: partial sums (doubles)
-// and output tiles (arrival counters).
-size_t splitk_need(const kfmm_plan* p, size_t* tiles = nullptr) {
-  size_t n = 0, t = 0;
+// Split-K scratch the plan's level products need (doubles).
+size_t splitk_need(const kfmm_plan* p) {
+  size_t n = 0;
   for (const auto* v : {&p->up_gemms, &p->down_gemms})
     for (const GemmBatch& g : *v)
-      if (g.nsplit > 1) {
-        n = std::max(n, (size_t)g.nsplit * g.ncol * g.M);
-        t = std::max(t, (size_t)g.chunks * ((g.ncol + kGemmBN - 1) / kGemmBN));
-      }
-  if (tiles) *tiles = t;
+      if (g.nsplit > 1) n = std::max(n, (size_t)g.nsplit * g.ncol * g.M);
   return n;
 }
 
-// Split-K buffers at least as large as the level products need.
+// Split-K partial-sum buffer at least as large as the level products need.
 kfmm_status ensure_splitk(kfmm_plan* p) {
-  size_t tiles = 0;
-  const size_t need = splitk_need(p, &tiles);
+  const size_t need = splitk_need(p);
   if (need > p->splitk_doubles) {
     dfree(p, p->splitk);
     KF_TRY(dalloc(p, &p->splitk, need));
     p->splitk_doubles = need;
   }
-  if (tiles > p->gemm_tiles_n) {
-    dfree(p, p->gemm_tiles);
-    KF_TRY(dalloc(p, &p->gemm_tiles, tiles));
-    KF_CUDA(cudaMemset(p->gemm_tiles, 0, sizeof(int) * tiles));
-    p->gemm_tiles_n = tiles;
-  }
   return KFMM_OK;
+}
+
+// Kernel launches of one kfmm_run (kfmm_plan_stats.launches).
+void count_launches(kfmm_plan* p) {
+  int reduces = 0;
+  for (const auto* v : {&p->up_gemms, &p->down_gemms})
+    for (const GemmBatch& g : *v) reduces += g.nsplit > 1;
+  p->stats.launches = reduces + (p->n_s2m > 0) + (int)p->up_gemms.size() + (p->n_fft > 0) +
+                      (p->prec == KFMM_MIXED ? (p->n_pairs > 0) + (p->n_singles > 0)
+                                             : (p->n_groups > 0)) +
+                      (p->n_ifft > 0) + (p->n_s2l > 0) +
+                      (int)p->down_gemms.size() + (p->n_nf > 0) +
+                      (p->prec == KFMM_MIXED ? 0 : 1);  // the plain form's scatter pass
 }
 
 kfmm_status add_gemm(kfmm_plan* p, std::vector<GemmBatch>& out, const double* A, int M, int K,
@@ -290,10 +289,16 @@ kfmm_status add_gemm(kfmm_plan* p, std::vector<GemmBatch>& out, const double* A,
 kfmm_status launch_gemms(const kfmm_plan* p, const std::vector<GemmBatch>& gs, cudaStream_t st) {
   for (const GemmBatch& b : gs) {
     GemmArgs a{b.A, b.M, b.K, b.ksplit, b.nsplit > 1 ? p->splitk : nullptr, b.B, b.boff, b.C,
-               b.coff, b.alpha, b.alpha_const, b.ncol, b.accumulate, p->gemm_tiles};
+               b.coff, b.alpha, b.alpha_const, b.ncol, b.accumulate};
     dim3 grid(b.chunks, (b.ncol + kGemmBN - 1) / kGemmBN, b.nsplit);
     gemm_fp64_dmma_kernel<<<grid, kGemmThreads, kGemmSmemBytes, st>>>(a, b.mrows);
     KF_CHECK_LAUNCH("gemm_fp64_dmma_kernel");
+    if (b.nsplit > 1) {
+      const size_t total = (size_t)b.ncol * b.M;
+      const int blocks = (int)std::min<size_t>((total + 255) / 256, 4 * (size_t)p->num_sms);
+      gemm_splitk_reduce_kernel<<<blocks, 256, 0, st>>>(a, b.nsplit);
+      KF_CHECK_LAUNCH("gemm_splitk_reduce_kernel");
+    }
   }
   return KFMM_OK;
 }
@@ -1038,12 +1043,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   p->stats.P = P;
   p->stats.Q = Q;
   p->stats.F = F;
-  p->stats.launches = (p->n_s2m > 0) + (int)p->up_gemms.size() + (p->n_fft > 0) +
-                      (p->prec == KFMM_MIXED ? (p->n_pairs > 0) + (p->n_singles > 0)
-                                             : (p->n_groups > 0)) +
-                      (p->n_ifft > 0) + (p->n_s2l > 0) +
-                      (int)p->down_gemms.size() + (p->n_nf > 0) +
-                      (p->prec == KFMM_MIXED ? 0 : 1);  // the plain form's scatter pass
+  count_launches(p);
   for (int i = 0; i < kfmm_plan::kMarks; ++i) KF_CUDA(cudaEventCreate(&p->ev[i]));
   KF_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
   KF_CUDA(cudaStreamCreateWithFlags(&p->d2h, cudaStreamNonBlocking));
@@ -1199,6 +1199,7 @@ kfmm_status kfmm_plan_set_tuning(kfmm_plan* p, const kfmm_tuning* tuning) {
     for (auto* v : {&p->up_gemms, &p->down_gemms})
       for (GemmBatch& g : *v) choose_split(p, g);
     KF_TRY(ensure_splitk(p));
+    count_launches(p);
   }
   return KFMM_OK;
 }
