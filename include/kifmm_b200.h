@@ -136,12 +136,19 @@ kfmm_status kfmm_plan_create_with_operators(const kfmm_tree_desc* tree, int np,
  *               pairs, else 6)
  *   had_windows mixed Hadamard: sibling windows per warp of a CTA, 1..8
  *               (automatic: the shortest span in waves of one CTA per SM)
- *   splitk_max  level products: largest split-K factor (automatic: K / 64) */
+ *   splitk_max  level products: largest split-K factor (automatic:
+ *               max(8, K / 64))
+ *   had_tensor  mixed Hadamard on the tcgen05 tensor cores (TF32, three
+ *               passes) for levels whose boxes are all present: 2 every
+ *               complete level; 0 automatic and 1 none (the CUDA-core kernels,
+ *               measured faster on B200); fixed when the plan is created
+ *               (kfmm_plan_set_tuning keeps the creation's choice) */
 typedef struct {
   int nf_blocks;
   int job_rows;
   int had_windows;
   int splitk_max;
+  int had_tensor;
 } kfmm_tuning;
 
 /* kfmm_plan_create_with_operators with launch choices; ops and tuning may be
@@ -247,6 +254,7 @@ typedef struct {
   double spectra_bytes; /* source + target spectra bytes, one pass each */
   int num_nodes, P, Q, F;
   int launches;        /* kernels one kfmm_run launches */
+  int tensor_levels;   /* levels whose Hadamard runs on the tcgen05 tensor cores */
 } kfmm_stats;
 kfmm_status kfmm_plan_stats(const kfmm_plan* plan, kfmm_stats* stats);
 

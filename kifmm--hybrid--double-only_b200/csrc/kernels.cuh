@@ -1464,6 +1464,8 @@ __global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(
   }
 }
 
+#include "hadamard_tc.cuh"
+
 // ---------------------------------------------------------------------------
 // Point reordering (fmm/evaluate.cc:14-52 on the host in the reference) and
 // the final scatter to original order (copy_trg_val, fmm/cuda.cu:2543-2565).

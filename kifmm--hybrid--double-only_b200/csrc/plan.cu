@@ -130,6 +130,12 @@ struct kfmm_plan {
       *single_members = nullptr;
   int n_pairs = 0, n_singles = 0;
   int pair_per_block = 0;
+  // tensor-core Hadamard (mixed form) on the complete levels it takes: levels,
+  // box -> node maps and the MMAs' B operands; the spectra, the error flag and
+  // the unit counter are filled in at launch
+  HadTcParams tc{};
+  int n_tc_levels = 0;
+  int* tc_counter = nullptr;
   kfmm_stats stats{};
   int num_sms = 148;
   double* splitk = nullptr;   // split-K partial sums, shared by the level GEMMs
@@ -246,10 +252,11 @@ void count_launches(kfmm_plan* p) {
   int reduces = 0;
   for (const auto* v : {&p->up_gemms, &p->down_gemms})
     for (const GemmBatch& g : *v) reduces += g.nsplit > 1;
+  p->stats.tensor_levels = p->n_tc_levels;
   p->stats.launches = reduces + (p->n_s2m > 0) + (int)p->up_gemms.size() + (p->n_fft > 0) +
                       (p->prec == KFMM_MIXED ? (p->n_pairs > 0) + (p->n_singles > 0)
                                              : (p->n_groups > 0)) +
-                      (p->n_ifft > 0) + (p->n_s2l > 0) +
+                      (p->n_tc_levels > 0) + (p->n_ifft > 0) + (p->n_s2l > 0) +
                       (int)p->down_gemms.size() + (p->n_nf > 0) +
                       (p->prec == KFMM_MIXED ? 0 : 1);  // the plain form's scatter pass
 }
@@ -504,7 +511,8 @@ void set_had_blocks(kfmm_plan* p) {
 kfmm_status check_tuning(const kfmm_tuning* t) {
   if (t && (t->nf_blocks < 0 || t->nf_blocks > 6 || (t->nf_blocks > 0 && t->nf_blocks < 5) ||
             t->job_rows < 0 || t->job_rows > kMaxSlots || t->had_windows < 0 ||
-            t->had_windows > 8 || t->splitk_max < 0)) {
+            t->had_windows > 8 || t->splitk_max < 0 || t->had_tensor < 0 ||
+            t->had_tensor > 2)) {
     set_error("kfmm_tuning: tuning value out of range");
     return KFMM_ERR_INVALID;
   }
@@ -844,6 +852,97 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       gparent.push_back(pn);
     }
     p->n_groups = (int)mem.size() / 8;
+    // Mixed form: levels whose boxes are all present go to the tensor-core
+    // kernel (hadamard_tc_kernel); it reads box -> node maps of the level
+    std::vector<char> tc_level(maxd + 1, 0);
+    // (only when the tuning asks for it: on B200 the CUDA-core kernels below
+    // measured faster, 1.53 against 3.21 ms at 4M points, NP=6: with 16
+    // output columns per frequency each MMA streams its whole A tile for 16
+    // columns, a sixteenth of the tensor cores' rate)
+    if (p->prec == KFMM_MIXED && p->n_groups && p->tune.had_tensor == 2) {
+      std::vector<int> groups_at(maxd + 1, 0);
+      for (int g = 0; g < p->n_groups; ++g) ++groups_at[d->depth[gparent[g]] + 1];
+      for (int cd = 2; cd <= std::min(maxd, 7); ++cd) {
+        const long long nb = 1ll << (3 * cd);
+        if (groups_at[cd] == 0 || (long long)at[cd].size() != nb) continue;
+        if (p->n_tc_levels == kTcMaxLevels) break;
+        tc_level[cd] = 1;
+        const int n = 1 << cd;
+        std::vector<int> sm(nb, -1), tm(nb, -1);
+        for (const auto& kv : at[cd]) {
+          const int node = kv.second;
+          const int x = d->path[3 * node], y = d->path[3 * node + 1], z = d->path[3 * node + 2];
+          const size_t q = ((size_t)z * n + y) * n + x;
+          if (has_src(node)) sm[q] = node;
+          if (has_trg(node) && d->v_ptr[node + 1] > d->v_ptr[node]) tm[q] = node;
+        }
+        TcLevel& L = p->tc.lv[p->n_tc_levels++];
+        L.n = n;
+        L.ntx = (n / 2 + kTcGX - 1) / kTcGX;
+        L.nty = (n / 2 + kTcGY - 1) / kTcGY;
+        L.col0 = p->tc.cols;
+        p->tc.cols += L.ntx * L.nty;
+        int* dm = nullptr;
+        KF_TRY(upload(p, &dm, sm));
+        L.srcmap = dm;
+        KF_TRY(upload(p, &dm, tm));
+        L.trgmap = dm;
+      }
+      if (p->n_tc_levels) {
+        // B operands per frequency, in the order the kernel issues its MMAs
+        // (plane wz, row pair q, MMA i of the pair): for MMA i its two K
+        // chunks (window row, box pair); per chunk the K elements re S(wx),
+        // im S(wx), re S(wx+1), im S(wx+1); columns n = 2 c + (re | im of E_c).
+        // B is stored K-major as core matrices [n block][K chunk][8 rows][16 B]
+        // (LBO 128 B, SBO 256 B), TF32 hi = rn(t), lo = rn(t - hi).
+        auto tf32 = [](float x) {
+          unsigned u;
+          std::memcpy(&u, &x, 4);
+          u = (u + 0x1000u) & 0xffffe000u;  // nearest, ties away from zero
+          float r;
+          std::memcpy(&r, &u, 4);
+          return r;
+        };
+        std::vector<float> bt((size_t)F * 2 * kTcMma * 128, 0.f);
+        for (int f = 0; f < F; ++f)
+          for (int j = 0; j < kTcMma; ++j) {
+            const int wz = j / 9, q = (j % 9) / 3, i = j % 3;
+            for (int kc = 0; kc < 2; ++kc) {
+              // (row, box pair) of this chunk: i 0 -> (2q, 0), (2q, 1); i 1 -> (2q, 2),
+              // (2q + 1, 0); i 2 -> (2q + 1, 1), (2q + 1, 2)
+              const int slot = 2 * i + kc;
+              const int wy = 2 * q + slot / 3, pr = slot % 3;
+              for (int nrow = 0; nrow < 16; ++nrow) {
+                const int c = nrow >> 1, o = nrow & 1;
+                for (int e = 0; e < 4; ++e) {
+                  const int wx = 2 * pr + (e >> 1), part = e & 1;
+                  const int dx = wx - 2 - (c >> 2), dy = wy - 2 - ((c >> 1) & 1),
+                            dz = wz - 2 - (c & 1);
+                  const int id = (dx + 3) + 7 * (dy + 3) + 49 * (dz + 3);
+                  float tr = 0.f, ti = 0.f;
+                  if (!adjacent(id)) {
+                    tr = (float)op.ue2dc[2 * ((size_t)id * F + f)];
+                    ti = (float)op.ue2dc[2 * ((size_t)id * F + f) + 1];
+                  }
+                  const float v = part == 0 ? (o == 0 ? tr : ti) : (o == 0 ? -ti : tr);
+                  const float hi = tf32(v), lo = tf32(v - hi);
+                  const size_t at0 = (((size_t)f * 2) * kTcMma + j) * 128 +
+                                     ((nrow >> 3) * 2 + kc) * 32 + (nrow & 7) * 4 + e;
+                  bt[at0] = hi;
+                  bt[at0 + (size_t)kTcMma * 128] = lo;
+                }
+              }
+            }
+          }
+        float* db = nullptr;
+        KF_TRY(upload(p, &db, bt));
+        p->tc.btab = (const unsigned char*)db;
+        p->tc.nn = nn;
+        p->tc.F = F;
+        p->tc.nlevels = p->n_tc_levels;
+        KF_TRY(dalloc(p, &p->tc_counter, 1));
+      }
+    }
     if (p->prec == KFMM_MIXED && p->n_groups) {
       // pair groups whose parents are x-neighbours (x even, x + 1): their
       // windows share 4 of 6 x-positions and form one 8 x 6 x 6 window
@@ -854,6 +953,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
         gat[d->depth[pn]][key_of(d->path[3 * pn], d->path[3 * pn + 1], d->path[3 * pn + 2])] = g;
       }
       std::vector<char> used(p->n_groups, 0);
+      for (int g = 0; g < p->n_groups; ++g) used[g] = tc_level[d->depth[gparent[g]] + 1];
       std::vector<int> pwin, pmem, swin, smem;
       for (int g = 0; g < p->n_groups; ++g) {
         if (used[g]) continue;
@@ -1014,6 +1114,8 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
 
   KF_CUDA(cudaFuncSetAttribute(gemm_fp64_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kGemmSmemBytes));
+  KF_CUDA(cudaFuncSetAttribute(hadamard_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kTcSmemBytes));
   KF_CUDA(cudaFuncSetAttribute(hadamard_fp32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kHad32TileBytes));
   KF_CUDA(cudaFuncSetAttribute(hadamard_fp32_pair_kernel,
@@ -1191,6 +1293,7 @@ kfmm_status kfmm_plan_set_tuning(kfmm_plan* p, const kfmm_tuning* tuning) {
   KF_TRY(check_tuning(tuning));
   const kfmm_tuning old = p->tune;
   p->tune = tuning ? *tuning : kfmm_tuning{};
+  p->tune.had_tensor = old.had_tensor;  // the levels' kernels are chosen at creation
   KF_CUDA(cudaDeviceSynchronize());  // no launch of the plan may still read what changes
   if (p->tune.job_rows != old.job_rows || p->tune.nf_blocks != old.nf_blocks)
     KF_TRY(build_nf_jobs(p));
@@ -1309,6 +1412,17 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
         dim3 grid((p->n_singles + gpb - 1) / gpb, p->Fpad / kFB);
         hadamard_fp32_kernel<<<grid, kHad32Threads, kHad32TileBytes, S(stream)>>>(h);
         KF_CHECK_LAUNCH("hadamard_fp32_kernel");
+      }
+      if (p->n_tc_levels) {
+        KF_CUDA(cudaMemsetAsync(p->tc_counter, 0, sizeof(int), S(stream)));
+        HadTcParams h = p->tc;
+        h.spec = (const float2*)p->spec;
+        h.effv = (float2*)p->effv;
+        h.next_unit = p->tc_counter;
+        h.error = p->d_error;
+        h.wait_limit = p->wait_limit;
+        hadamard_tc_kernel<<<p->num_sms, kTcThreads, kTcSmemBytes, S(stream)>>>(h);
+        KF_CHECK_LAUNCH("hadamard_tc_kernel");
       }
     } else {
       HadamardParams h{p->nn, p->n_groups, kHadGroupsPerBlock, p->win, p->members,

@@ -298,6 +298,72 @@ def test_mixed_downward_check_vs_plain(K, cuda_ok, case):
     assert len(nodes) > 0 and e <= 2e-5
 
 
+TENSOR_CASES = [("uniform", 65536, 128, 6, 0, 2), ("uniform", 262144, 64, 4, 0, 2),
+                ("uniform", 300000, 32, 3, 1, 2), ("uniform", 150000, 16, 5, 0, 2)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", TENSOR_CASES, ids=lambda c: _ids(c) + f"-tc{c[5]}")
+def test_tensor_core_hadamard(K, oracle_mod, cuda_ok, case):
+    """The mixed form's Hadamard on the tcgen05 tensor cores (TF32 hi/lo
+    split, three passes, FP32 accumulation in tensor memory) for the levels
+    whose boxes are all present, against the same plan with the CUDA-core
+    FP32 kernels everywhere (had_tensor 1): downward check potentials per
+    node within 2e-5 of the plain FP64 path (the CUDA-core form's bar),
+    potentials within 1e-6 (rel-L2) of the CUDA-core mixed form, and the
+    reference's check (rel-L2 against the exact direct sum) within 2x the
+    plain path's error (had_tensor 2: every complete level)."""
+    dist, n, ppb, np_, coincide, mode = case
+    pts = K.generate_points(n, dist, coincide, 26, 300)
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], ppb)
+    P, _, _ = K.sizes(np_)
+    nn = tree.desc.num_nodes
+    res = {}
+    for name, prec, tun in (("plain", K.PLAIN_FP64, None), ("cuda", K.MIXED, None),
+                            ("tensor", K.MIXED, {"had_tensor": mode})):
+        plan = K.Plan(tree, np_, prec, tuning=tun)
+        pot = plan.evaluate(pts)
+        res[name] = (pot, plan.read(1, nn * P), plan.stats()["tensor_levels"])
+        plan.close()
+    assert res["cuda"][2] == 0 and res["tensor"][2] >= 1, res["tensor"][2]
+    tag = tree.array("tag")
+    dplain = res["plain"][1]
+    nodes = np.where(((tag & 2) != 0) & (np.abs(dplain.reshape(-1, P)).max(axis=1) > 0))[0]
+    e_tc = _node_err(res["tensor"][1], dplain, P, nodes)
+    e_cc = _node_err(res["cuda"][1], dplain, P, nodes)
+    tc, cc, plain = res["tensor"][0], res["cuda"][0], res["plain"][0]
+    vs_cuda = np.linalg.norm(tc - cc) / np.linalg.norm(cc)
+    ids = pts["check_ids"]
+    d = oracle_mod.direct(pts["tx"][ids], pts["ty"][ids], pts["tz"][ids], pts["sx"], pts["sy"],
+                          pts["sz"], pts["den"])
+    e_plain = np.linalg.norm(plain[ids] - d) / np.linalg.norm(d)
+    e_tens = np.linalg.norm(tc[ids] - d) / np.linalg.norm(d)
+    print(f"{_ids(case)} tc{mode}: {res['tensor'][2]} tensor levels; dchk vs plain: tensor "
+          f"{e_tc:.2e}, CUDA cores {e_cc:.2e}; potentials tensor vs CUDA cores {vs_cuda:.2e}; "
+          f"rel-L2 vs direct: plain {e_plain:.3e} tensor {e_tens:.3e}")
+    assert np.all(np.isfinite(tc))
+    assert e_tc <= 2e-5
+    assert vs_cuda <= 1e-6
+    assert e_tens <= 2.0 * e_plain
+
+
+@pytest.mark.gpu
+def test_tensor_choice_fixed_at_creation(K, cuda_ok):
+    """kfmm_plan_set_tuning leaves the tensor-core choice as created, and
+    re-running after other changes gives the same potentials bit for bit."""
+    pts = K.generate_points(262144, "uniform", 0, 5)
+    tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], 64)
+    assert K.Plan(tree, 4, K.MIXED).stats()["tensor_levels"] == 0  # automatic: CUDA cores
+    plan = K.Plan(tree, 4, K.MIXED, tuning={"had_tensor": 2})
+    levels = plan.stats()["tensor_levels"]
+    assert levels == 3  # depths 2, 3 and 4 are complete
+    want = plan.evaluate(pts)
+    plan.set_tuning({"had_tensor": 1, "job_rows": 3})
+    assert plan.stats()["tensor_levels"] == levels
+    assert np.array_equal(plan.evaluate(pts), want)
+    plan.close()
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [1, 2, 9, 100, 700])
 def test_tiny_inputs(K, oracle_mod, cuda_ok, n):
