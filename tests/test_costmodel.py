@@ -91,12 +91,14 @@ def test_gpu_training_fits(K, cuda_ok):
 @pytest.mark.gpu
 @pytest.mark.skipif(not os.path.exists(HARVEST), reason="no harvested dataset")
 def test_model_picks_near_sweep_best(K, cuda_ok):
-    """Held-out clouds of the harvest (every fifth): the pick over (leaf
-    size, near-field configuration) is within 5% of the measured sweep's best
-    on average, and, with the measured fallback, on at least 90% of the
-    clouds one by one; both beat the fixed default (512 per leaf, automatic
-    configuration), which is what the network gains over the method without
-    it."""
+    """Held-out clouds of the harvest (every fifth: 400 of 2,000): the pick
+    over (leaf size, near-field configuration) is within 5% of the measured
+    sweep's best on average and on at least 85% of the clouds one by one
+    (measured on a B200: 1.02 on average, 90% of the clouds; Gaussian
+    clusters, the hard case, 1.03-1.04), and, with the measured fallback, on
+    at least 90% (measured 96%); both beat the fixed default (512 per leaf,
+    automatic configuration: 1.31), which is what the network gains over the
+    method without it."""
     from kifmm_b200 import costmodel
     data = dict(np.load(HARVEST))
     train = data["cloud"] % 5 != 0
@@ -118,6 +120,7 @@ def test_model_picks_near_sweep_best(K, cuda_ok):
           f"instead of {len(costmodel.LEAF_SIZES) * len(costmodel.CONFIGS)} times); default 512 "
           f"/ sweep best {dflt:.4f}")
     assert pick <= 1.05
+    assert within >= 0.85  # cloud by cloud, not only on average
     assert fb <= pick
     assert within_fb >= 0.90
     assert pick < dflt
