@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=BATCH_SOLVES)
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="profile one form only (no JSON line)")
+    ap.add_argument("--had-tensor", action="store_true",
+                    help="with --only mixed: the Hadamard on the tensor cores (kfmm_tuning.had_tensor 2)")
     return ap.parse_args()
 
 
@@ -430,7 +432,8 @@ def main():
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
     if args.only:
-        pl = K.Plan(tree, NP, K.MIXED if args.only == "mixed" else K.PLAIN_FP64)
+        pl = K.Plan(tree, NP, K.MIXED if args.only == "mixed" else K.PLAIN_FP64,
+                    tuning={"had_tensor": 2} if args.had_tensor else None)
         pl.set_points(pts, sh)
         for _ in range(args.warmup + args.steps):
             pl.run(sh)
