@@ -142,13 +142,23 @@ kfmm_status kfmm_plan_create_with_operators(const kfmm_tree_desc* tree, int np,
  *               passes) for levels whose boxes are all present: 2 every
  *               complete level; 0 automatic and 1 none (the CUDA-core kernels,
  *               measured faster on B200); fixed when the plan is created
- *               (kfmm_plan_set_tuning keeps the creation's choice) */
+ *               (kfmm_plan_set_tuning keeps the creation's choice)
+ *   cpu_share_ppm hybrid evaluation (fmm/run--hybrid2.cu:25-47, where the
+ *               host's cores run the U list while the GPU runs up, V and
+ *               down): the host CPU takes the U-list point pairs of the
+ *               cheapest target leaves up to this share of all of them, in
+ *               parts per million (1,000,000: the whole U list, the
+ *               reference's schedule), in FP64, while the GPU runs the rest;
+ *               fixed at creation.  Such plans evaluate through
+ *               kfmm_evaluate only (kfmm_run, kfmm_evaluate_async,
+ *               kfmm_ulist_calc and batches refuse them). */
 typedef struct {
   int nf_blocks;
   int job_rows;
   int had_windows;
   int splitk_max;
   int had_tensor;
+  int cpu_share_ppm;
 } kfmm_tuning;
 
 /* kfmm_plan_create_with_operators with launch choices; ops and tuning may be
@@ -208,7 +218,11 @@ kfmm_status kfmm_get_potentials_device(kfmm_plan* plan, double* pot_dev, void* s
 kfmm_status kfmm_set_wait_limit(kfmm_plan* plan, long long tries);
 
 /* End-to-end: host inputs (original order) -> host potentials
- * (synchronous; kfmm_evaluate_async followed by kfmm_evaluate_wait). */
+ * (synchronous; kfmm_evaluate_async followed by kfmm_evaluate_wait).  For a
+ * hybrid plan (kfmm_tuning.cpu_share_ppm > 0) the calling thread's OpenMP
+ * team sums the host's share of the U list in FP64 from the host arrays
+ * while the GPU works, and adds it to the downloaded potentials
+ * (fmm/run--hybrid2.cu:25-47). */
 kfmm_status kfmm_evaluate(kfmm_plan* plan, const double* sx, const double* sy,
                           const double* sz, const double* den, const double* tx,
                           const double* ty, const double* tz, double* pot, void* stream);
@@ -255,6 +269,7 @@ typedef struct {
   int num_nodes, P, Q, F;
   int launches;        /* kernels one kfmm_run launches */
   int tensor_levels;   /* levels whose Hadamard runs on the tcgen05 tensor cores */
+  double host_pairs;   /* U-list pairs the host sums (hybrid plans) */
 } kfmm_stats;
 kfmm_status kfmm_plan_stats(const kfmm_plan* plan, kfmm_stats* stats);
 

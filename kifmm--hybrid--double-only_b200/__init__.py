@@ -47,14 +47,15 @@ class OperatorSet(ctypes.Structure):
 class Tuning(ctypes.Structure):
     """kfmm_tuning: launch choices, 0 = the plan's automatic choice."""
     _fields_ = [(n, ctypes.c_int) for n in ("nf_blocks", "job_rows", "had_windows",
-                                             "splitk_max", "had_tensor")]
+                                             "splitk_max", "had_tensor", "cpu_share_ppm")]
 
 
 class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in ("u_pairs", "s2m_pairs", "s2l_pairs", "v_pairs",
                                                 "hadamard_cmacs", "gemm_flops",
                                                 "spectra_bytes")] + [
-        (n, ctypes.c_int) for n in ("num_nodes", "P", "Q", "F", "launches", "tensor_levels")]
+        (n, ctypes.c_int) for n in ("num_nodes", "P", "Q", "F", "launches", "tensor_levels")] + [
+        ("host_pairs", ctypes.c_double)]
 
 
 def lib():

@@ -20,6 +20,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -93,6 +94,7 @@ struct kfmm_plan {
   size_t cplx = sizeof(double2);
   // operators
   double *d_uc2ue = nullptr, *d_ue2uc = nullptr, *d_dc2de = nullptr, *d_de2dc_stack = nullptr;
+  double* d_m2m = nullptr;  // mixed form: UC2UE x UE2UC, P x 8P (one product per M2M level)
   void* d_trans = nullptr;
   double *d_sp_ue = nullptr, *d_sp_uc = nullptr, *d_sp_de = nullptr, *d_sp_dc = nullptr;
   float *d_spf_ue = nullptr, *d_spf_de = nullptr;
@@ -136,6 +138,18 @@ struct kfmm_plan {
   HadTcParams tc{};
   int n_tc_levels = 0;
   int* tc_counter = nullptr;
+  // hybrid evaluation (kfmm_tuning.cpu_share_ppm): the host evaluates the
+  // U lists of these target leaves; their GPU near-field jobs skip the U
+  // entries.  Per leaf: its targets host_trg[tbeg, tbeg + tcnt) (original
+  // indices) and its U entries host_u[ubeg, uend), each a range of host_src
+  // (the original indices of one source leaf's points).
+  struct HostLeaf {
+    int tbeg, tcnt, ubeg, uend;
+  };
+  std::vector<HostLeaf> host_leaves;
+  std::vector<int> host_trg, host_src;
+  std::vector<int2> host_u;
+  double host_pairs = 0.0;
   kfmm_stats stats{};
   int num_sms = 148;
   double* splitk = nullptr;   // split-K partial sums, shared by the level GEMMs
@@ -253,6 +267,7 @@ void count_launches(kfmm_plan* p) {
   for (const auto* v : {&p->up_gemms, &p->down_gemms})
     for (const GemmBatch& g : *v) reduces += g.nsplit > 1;
   p->stats.tensor_levels = p->n_tc_levels;
+  p->stats.host_pairs = p->host_pairs;
   p->stats.launches = reduces + (p->n_s2m > 0) + (int)p->up_gemms.size() + (p->n_fft > 0) +
                       (p->prec == KFMM_MIXED ? (p->n_pairs > 0) + (p->n_singles > 0)
                                              : (p->n_groups > 0)) +
@@ -512,7 +527,7 @@ kfmm_status check_tuning(const kfmm_tuning* t) {
   if (t && (t->nf_blocks < 0 || t->nf_blocks > 6 || (t->nf_blocks > 0 && t->nf_blocks < 5) ||
             t->job_rows < 0 || t->job_rows > kMaxSlots || t->had_windows < 0 ||
             t->had_windows > 8 || t->splitk_max < 0 || t->had_tensor < 0 ||
-            t->had_tensor > 2)) {
+            t->had_tensor > 2 || t->cpu_share_ppm < 0 || t->cpu_share_ppm > 1000000)) {
     set_error("kfmm_tuning: tuning value out of range");
     return KFMM_ERR_INVALID;
   }
@@ -597,6 +612,19 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   // --- operators and surfaces
   KF_TRY(upload(p, &p->d_uc2ue, op.uc2ue));
   KF_TRY(upload(p, &p->d_ue2uc, op.ue2uc));  // Q x 8P, the 8 blocks side by side
+  if (p->prec == KFMM_MIXED) {
+    // M2M as one operator: uden_parent = 2^-d UC2UE (sum_c UE2UC_c 2^(d+1) uden_c)
+    // = 2 (UC2UE UE2UC) [uden_c] (fmm/omp_sse_block.cc:103-155), the product
+    // formed once here in FP64 (column-major, P x 8P)
+    std::vector<double> m((size_t)P * 8 * P, 0.0);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < 8 * P; ++k)
+      for (int q = 0; q < Q; ++q) {
+        const double u = op.ue2uc[(size_t)k * Q + q];
+        for (int i = 0; i < P; ++i) m[(size_t)k * P + i] += op.uc2ue[(size_t)q * P + i] * u;
+      }
+    KF_TRY(upload(p, &p->d_m2m, m));
+  }
   KF_TRY(upload(p, &p->d_dc2de, op.dc2de));
   {
     std::vector<double> st((size_t)8 * P * P);  // 8P x P: the 8 blocks stacked
@@ -769,7 +797,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     for (int i = 0; i < nn; ++i)
       if (!is_leaf(i) && has_src(i)) par[d->depth[i]].push_back(i);
     for (int dd = 0; dd <= maxd; ++dd) maxpar = std::max(maxpar, (int)par[dd].size());
-    KF_TRY(dalloc(p, &p->chk_m, (size_t)maxpar * Q));
+    if (p->prec != KFMM_MIXED) KF_TRY(dalloc(p, &p->chk_m, (size_t)maxpar * Q));
     // Equivalent densities of depth 0 and 1 nodes are never read: V lists
     // start at depth 2 and W-list nodes lie below a depth >= 1 leaf's
     // colleagues, so at depth >= 2.  M2M stops at parents of depth 2.
@@ -782,10 +810,17 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
         b2.push_back((int)k * Q);
         c2.push_back(par[dd][k] * P);
       }
-      KF_TRY(add_gemm(p, p->up_gemms, p->d_ue2uc, Q, 8 * P, p->uden, b1, p->chk_m, c1, nullptr,
-                      std::ldexp(1.0, dd + 1), 0));
-      KF_TRY(add_gemm(p, p->up_gemms, p->d_uc2ue, P, Q, p->chk_m, b2, p->uden, c2, nullptr,
-                      std::ldexp(1.0, -dd), 0));
+      if (p->prec == KFMM_MIXED) {
+        // one product of the fused operator: half the flops of the two
+        // (P x 8P against Q x 8P + P x Q), no intermediate check potentials
+        KF_TRY(add_gemm(p, p->up_gemms, p->d_m2m, P, 8 * P, p->uden, b1, p->uden, c2, nullptr,
+                        2.0, 0));
+      } else {
+        KF_TRY(add_gemm(p, p->up_gemms, p->d_ue2uc, Q, 8 * P, p->uden, b1, p->chk_m, c1, nullptr,
+                        std::ldexp(1.0, dd + 1), 0));
+        KF_TRY(add_gemm(p, p->up_gemms, p->d_uc2ue, P, Q, p->chk_m, b2, p->uden, c2, nullptr,
+                        std::ldexp(1.0, -dd), 0));
+      }
     }
   }
 
@@ -1081,10 +1116,51 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       all_pairs += ns * d->trg_num[t];
     }
     p->nf_w_heavy = w_pairs > 0.01 * (all_pairs + w_pairs);
+    // Hybrid: the host takes the U lists of the cheapest target leaves (by
+    // U-list pairs, ties in node order) up to cpu_share_ppm of all U pairs.
+    std::vector<char> on_host(nn, 0);
+    if (p->tune.cpu_share_ppm > 0) {
+      std::vector<std::pair<double, int>> cost;
+      for (int t = 0; t < nn; ++t) {
+        if (!is_leaf(t) || !has_trg(t) || d->trg_num[t] == 0) continue;
+        double ns = 0;
+        for (int k = d->u_ptr[t]; k < d->u_ptr[t + 1]; ++k) ns += d->src_num[d->u_idx[k]];
+        cost.push_back({ns * d->trg_num[t], t});
+      }
+      std::stable_sort(cost.begin(), cost.end(),
+                       [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+                         return a.first < b.first;
+                       });
+      const double want = all_pairs * (p->tune.cpu_share_ppm * 1e-6);
+      std::vector<int> src_at(nn, -1);  // source leaf -> its range in host_src
+      for (const auto& c : cost) {
+        if (p->host_pairs + c.first > want && p->tune.cpu_share_ppm < 1000000) break;
+        const int t = c.second;
+        on_host[t] = 1;
+        p->host_pairs += c.first;
+        kfmm_plan::HostLeaf L;
+        L.tbeg = (int)p->host_trg.size();
+        L.tcnt = d->trg_num[t];
+        for (int i = 0; i < L.tcnt; ++i) p->host_trg.push_back(d->trg_perm[d->trg_beg[t] + i]);
+        L.ubeg = (int)p->host_u.size();
+        for (int k = d->u_ptr[t]; k < d->u_ptr[t + 1]; ++k) {
+          const int s = d->u_idx[k];
+          if (src_at[s] < 0) {
+            src_at[s] = (int)p->host_src.size();
+            for (int i = 0; i < d->src_num[s]; ++i)
+              p->host_src.push_back(d->src_perm[d->src_beg[s] + i]);
+          }
+          p->host_u.push_back(make_int2(src_at[s], src_at[s] + d->src_num[s]));
+        }
+        L.uend = (int)p->host_u.size();
+        p->host_leaves.push_back(L);
+      }
+    }
     for (int t = 0; t < nn; ++t) {
       if (!is_leaf(t) || !has_trg(t) || d->trg_num[t] == 0) continue;
       int e0 = (int)ent.size();
       for (int k = d->u_ptr[t]; k < d->u_ptr[t + 1]; ++k) ent.push_back(d->u_idx[k]);
+      const int e_after_u = (int)ent.size();
       for (int k = d->w_ptr[t]; k < d->w_ptr[t + 1]; ++k) {
         int s = d->w_idx[k];
         bool direct = is_leaf(s) && d->src_num[s] < P;  // fmm/omp.cc:675
@@ -1093,6 +1169,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       if (d->trg_num[t] < P)  // fmm/omp.cc:724
         for (int k = d->x_ptr[t]; k < d->x_ptr[t + 1]; ++k) ent.push_back(d->x_idx[k]);
       if (d->depth[t] >= 2) ent.push_back((2 << 28) | t);
+      if (on_host[t]) e0 = e_after_u;  // the host sums this leaf's U list
       int ns = 0;
       for (int k = e0; k < (int)ent.size(); ++k) ns += src_count(ent[k]);
       P2PJob j;
@@ -1294,6 +1371,7 @@ kfmm_status kfmm_plan_set_tuning(kfmm_plan* p, const kfmm_tuning* tuning) {
   const kfmm_tuning old = p->tune;
   p->tune = tuning ? *tuning : kfmm_tuning{};
   p->tune.had_tensor = old.had_tensor;  // the levels' kernels are chosen at creation
+  p->tune.cpu_share_ppm = old.cpu_share_ppm;  // and so is the host's share
   KF_CUDA(cudaDeviceSynchronize());  // no launch of the plan may still read what changes
   if (p->tune.job_rows != old.job_rows || p->tune.nf_blocks != old.nf_blocks)
     KF_TRY(build_nf_jobs(p));
@@ -1457,7 +1535,8 @@ kfmm_status kfmm_down_calc(kfmm_plan* p, void* stream) {
   return launch_gemms(p, p->down_gemms, S(stream));
 }
 
-kfmm_status kfmm_ulist_calc(kfmm_plan* p, void* stream) {
+namespace {
+kfmm_status near_field(kfmm_plan* p, void* stream) {
   if (!p || !p->have_trg || !p->have_src) {
     set_error("kfmm_ulist_calc: plan has no points");
     return KFMM_ERR_STATE;
@@ -1467,6 +1546,24 @@ kfmm_status kfmm_ulist_calc(kfmm_plan* p, void* stream) {
                       stream, "near field"));
   }
   return KFMM_OK;
+}
+
+// A hybrid plan's GPU near field leaves out the host's U lists: only
+// kfmm_evaluate, which adds them, may run it.
+kfmm_status refuse_hybrid(const kfmm_plan* p, const char* who) {
+  if (p && !p->host_leaves.empty()) {
+    set_error(std::string(who) +
+              ": the plan evaluates part of its U list on the host "
+              "(kfmm_tuning.cpu_share_ppm): use kfmm_evaluate");
+    return KFMM_ERR_UNSUPPORTED;
+  }
+  return KFMM_OK;
+}
+}  // namespace
+
+kfmm_status kfmm_ulist_calc(kfmm_plan* p, void* stream) {
+  KF_TRY(refuse_hybrid(p, "kfmm_ulist_calc"));
+  return near_field(p, stream);
 }
 
 kfmm_status kfmm_copy_trg_val(kfmm_plan* p, double* pot_host, void* stream) {
@@ -1526,17 +1623,19 @@ kfmm_status kfmm_run(kfmm_plan* p, void* stream) {
     set_error("kfmm_run: set sources and targets first");
     return KFMM_ERR_STATE;
   }
+  KF_TRY(refuse_hybrid(p, "kfmm_run"));
   KF_TRY(run_far_field(p, stream));
-  KF_TRY(kfmm_ulist_calc(p, stream));
+  KF_TRY(near_field(p, stream));
   mark(p, 8, S(stream));
   KF_TRY(kfmm_copy_trg_val(p, nullptr, stream));
   mark(p, 9, S(stream));
   return KFMM_OK;
 }
 
-kfmm_status kfmm_evaluate_async(kfmm_plan* p, const double* sx, const double* sy,
-                                const double* sz, const double* den, const double* tx,
-                                const double* ty, const double* tz, double* pot, void* stream) {
+namespace {
+kfmm_status evaluate_async(kfmm_plan* p, const double* sx, const double* sy, const double* sz,
+                           const double* den, const double* tx, const double* ty,
+                           const double* tz, double* pot, void* stream) {
   if (!p || !pot || !sx || !sy || !sz || !den || !tx || !ty || !tz) {
     set_error("kfmm_evaluate_async: null argument");
     return KFMM_ERR_INVALID;
@@ -1571,7 +1670,7 @@ kfmm_status kfmm_evaluate_async(kfmm_plan* p, const double* sx, const double* sy
   KF_TRY(run_far_field(p, stream));
   KF_CUDA(cudaStreamWaitEvent(st, p->ev_gtrg, 0));
   KF_CUDA(cudaStreamWaitEvent(st, p->ev_d2h, 0));
-  KF_TRY(kfmm_ulist_calc(p, stream));
+  KF_TRY(near_field(p, stream));
   mark(p, 8, st);
   KF_TRY(kfmm_copy_trg_val(p, nullptr, stream));
   mark(p, 9, st);
@@ -1583,6 +1682,42 @@ kfmm_status kfmm_evaluate_async(kfmm_plan* p, const double* sx, const double* sy
   KF_CUDA(cudaMemcpyAsync(pot, p->pot_orig, bt, cudaMemcpyDeviceToHost, p->d2h));
   KF_CUDA(cudaEventRecord(p->ev_d2h, p->d2h));
   return KFMM_OK;
+}
+
+// The host's share of a hybrid plan's U list (exact FP64 as fmm/omp.cc:259-283:
+// pairs at r = 0 skipped), from the original-order host arrays; add[j] for
+// target host_trg[j].
+void host_ulist(const kfmm_plan* p, const double* sx, const double* sy, const double* sz,
+                const double* den, const double* tx, const double* ty, const double* tz,
+                double* add) {
+  const int nl = (int)p->host_leaves.size();
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int h = 0; h < nl; ++h) {
+    const kfmm_plan::HostLeaf& L = p->host_leaves[h];
+    for (int i = 0; i < L.tcnt; ++i) {
+      const int t = p->host_trg[L.tbeg + i];
+      const double x = tx[t], y = ty[t], z = tz[t];
+      double sum = 0.0;
+      for (int e = L.ubeg; e < L.uend; ++e) {
+        const int2 r = p->host_u[e];
+        for (int k = r.x; k < r.y; ++k) {
+          const int s = p->host_src[k];
+          const double dx = x - sx[s], dy = y - sy[s], dz = z - sz[s];
+          const double r2 = dx * dx + dy * dy + dz * dz;
+          if (r2 > 0.0) sum += den[s] / std::sqrt(r2);
+        }
+      }
+      add[L.tbeg + i] = kOOFP * sum;
+    }
+  }
+}
+}  // namespace
+
+kfmm_status kfmm_evaluate_async(kfmm_plan* p, const double* sx, const double* sy,
+                                const double* sz, const double* den, const double* tx,
+                                const double* ty, const double* tz, double* pot, void* stream) {
+  KF_TRY(refuse_hybrid(p, "kfmm_evaluate_async"));
+  return evaluate_async(p, sx, sy, sz, den, tx, ty, tz, pot, stream);
 }
 
 kfmm_status kfmm_evaluate_join(kfmm_plan* p, void* stream) {
@@ -1615,8 +1750,22 @@ kfmm_status kfmm_evaluate(kfmm_plan* p, const double* sx, const double* sy, cons
     set_error("kfmm_evaluate: null argument");
     return KFMM_ERR_INVALID;
   }
-  KF_TRY(kfmm_evaluate_async(p, sx, sy, sz, den, tx, ty, tz, pot, stream));
-  return kfmm_evaluate_wait(p, stream);
+  if (p->host_leaves.empty()) {
+    KF_TRY(evaluate_async(p, sx, sy, sz, den, tx, ty, tz, pot, stream));
+    return kfmm_evaluate_wait(p, stream);
+  }
+  // hybrid: a host thread (and its OpenMP team) sums the host's U lists
+  // while this thread queues the GPU's work and waits for it (with pageable
+  // host arrays the copies themselves hold this thread); the sums are then
+  // added to the downloaded potentials
+  std::vector<double> add(p->host_trg.size());
+  std::thread host([&] { host_ulist(p, sx, sy, sz, den, tx, ty, tz, add.data()); });
+  kfmm_status st = evaluate_async(p, sx, sy, sz, den, tx, ty, tz, pot, stream);
+  if (st == KFMM_OK) st = kfmm_evaluate_wait(p, stream);
+  host.join();
+  if (st != KFMM_OK) return st;
+  for (size_t j = 0; j < add.size(); ++j) pot[p->host_trg[j]] += add[j];
+  return KFMM_OK;
 }
 
 kfmm_status kfmm_direct_evaluation(int nt, const double* tx, const double* ty, const double* tz,
@@ -1707,11 +1856,13 @@ kfmm_status kfmm_batch_create(kfmm_plan* const* plans, int nplans, int nstreams,
     return KFMM_ERR_INVALID;
   }
   *out = nullptr;
-  for (int i = 0; i < nplans; ++i)
+  for (int i = 0; i < nplans; ++i) {
     if (!plans[i] || !plans[i]->have_src || !plans[i]->have_trg) {
       set_error("kfmm_batch_create: plan " + std::to_string(i) + " is null or has no points");
       return KFMM_ERR_STATE;
     }
+    KF_TRY(refuse_hybrid(plans[i], "kfmm_batch_create"));
+  }
   nstreams = std::min(nstreams, nplans);
   kfmm_batch* b = new kfmm_batch();
   b->plans.assign(plans, plans + nplans);
