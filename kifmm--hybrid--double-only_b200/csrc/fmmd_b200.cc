@@ -3,6 +3,9 @@
 //   fmmd--b200 <#pts> {uniform,ellipseUniformAngles,ellipsoidSurface} <#pts-per-box>
 //   env NP (expansion order, default 6), NV (validation targets, default
 //   1000), C (1: targets are the sources), KFMM_MIXED=1 for the mixed form,
+//   KFMM_CPU_SHARE_PPM=<n> for the hybrid CPU+GPU evaluation (the host's
+//   cores sum that share of the U list, in parts per million; 1000000 is the
+//   schedule of the reference's fmmd--hybrid2, fmm/run--hybrid2.cu:25-47),
 //   KFMM_DUMP_POT=<file> to write the potentials (original order, raw doubles).
 //
 // Same sequence and output lines as fmm/driver.cc:211-371: seed 26, points,
@@ -12,6 +15,7 @@
 // sum runs on the GPU (kfmm_direct_evaluation).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -49,6 +53,7 @@ int main(int argc, char** argv) {
   const int np = env_int("NP", 6), nv = env_int("NV", 1000);
   const int coincide = env_int("C", 0) == 1 ? 1 : 0;
   const bool mixed = env_int("KFMM_MIXED", 0) == 1;
+  const int cpu_share = std::min(env_int("KFMM_CPU_SHARE_PPM", 0), 1000000);
 
   std::vector<double> sx(n), sy(n), sz(n), den(n), tx(n), ty(n), tz(n), pot(n);
   std::vector<int> ids(nv);
@@ -61,7 +66,10 @@ int main(int argc, char** argv) {
   CHECK(kfmm_tree_describe(tree, &desc));
   std::fprintf(stderr, "Preprocessing...\n");
   kfmm_plan* plan = nullptr;
-  CHECK(kfmm_plan_create(&desc, np, mixed ? KFMM_MIXED : KFMM_PLAIN_FP64, &plan));
+  kfmm_tuning tuning = {};
+  tuning.cpu_share_ppm = cpu_share;
+  CHECK(kfmm_plan_create_tuned(&desc, np, mixed ? KFMM_MIXED : KFMM_PLAIN_FP64, nullptr,
+                               cpu_share ? &tuning : nullptr, &plan));
   std::fprintf(stderr, "Finished setup.\n");
   std::fprintf(stderr, "Evaluation...\n");
   CHECK(kfmm_enable_timing(plan, 1));
@@ -81,7 +89,7 @@ int main(int argc, char** argv) {
                t_down = ms[3] * 1e-3, t_near = ms[4] * 1e-3, t_copy = ms[5] * 1e-3;
   const double total = t_up + t_v + t_x + t_down + t_near + t_copy;
   std::fprintf(stderr, "=== Statistics ===\n");
-  std::fprintf(stdout, "Code: b200-%s\n", mixed ? "mixed" : "fp64");
+  std::fprintf(stdout, "Code: b200-%s%s\n", mixed ? "mixed" : "fp64", cpu_share ? "-hybrid" : "");
   std::fprintf(stdout, "Floating-point word size: %lu bytes\n", (unsigned long)sizeof(double));
   std::fprintf(stderr, "== Timing for FMM3d ==\n");
   // U, W and the direct X list run in one fused kernel, reported as "U list"

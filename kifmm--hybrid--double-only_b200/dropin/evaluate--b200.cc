@@ -7,7 +7,10 @@
 // evaluation on the B200.  It compiles against the reference's headers; the
 // recipe is the fmmd--b200-dropin rule of oracle/Makefile.
 //
-// env: KFMM_MIXED=1 selects the mixed-precision form; KFMM_DUMP_POT=<file>
+// env: KFMM_MIXED=1 selects the mixed-precision form; KFMM_CPU_SHARE_PPM=<n>
+// the hybrid CPU+GPU evaluation (1000000: the whole U list on the host's
+// cores while the GPU runs the rest, the schedule of fmm/run--hybrid2.cu, so
+// this file then stands in for fmmd--hybrid2's run); KFMM_DUMP_POT=<file>
 // writes the potentials (original target order, raw doubles) after run(), so
 // tests can compare them per target with the reference's.
 #include <assert.h>
@@ -148,8 +151,15 @@ FMMWrapper_t* preproc(AllNodes* A) {
   FMMWrapper_t* F = (FMMWrapper_t*)calloc(1, sizeof(FMMWrapper_t));
   F->AN = A;
   F->num_trg = d.num_trg;
-  if (kfmm_plan_create_with_operators(&d, getenv__accuracy(), prec, &ops, &F->plan) != KFMM_OK)
-    fail("kfmm_plan_create_with_operators");
+  kfmm_tuning tuning;
+  memset(&tuning, 0, sizeof(tuning));
+  if (const char* h = getenv("KFMM_CPU_SHARE_PPM")) {
+    const long v = atol(h);
+    tuning.cpu_share_ppm = v < 0 ? 0 : (v > 1000000 ? 1000000 : (int)v);
+  }
+  if (kfmm_plan_create_tuned(&d, getenv__accuracy(), prec, &ops,
+                             tuning.cpu_share_ppm ? &tuning : NULL, &F->plan) != KFMM_OK)
+    fail("kfmm_plan_create_tuned");
   return F;
 }
 

@@ -11,7 +11,10 @@ same CLI and output lines.  For the same command line:
   operators (the drop-in), 5 x floor with this library's own pseudo-inverses;
 * they print the same "Relative error" (the driver's direct-sum check,
   fmm/driver.cc:142-206) as fmmd--omp, to the printed digits plus that floor;
-* the mixed form's printed error is at most 2x the reference's.
+* the mixed form's printed error is at most 2x the reference's;
+* fmmd--b200 with KFMM_CPU_SHARE_PPM=1000000 (the whole U list summed on the
+  host while the GPU runs the rest, fmm/run--hybrid2.cu) matches the
+  reference per target like the all-GPU run.
 
 The reference driver's check accumulates into an array it never zeroes
 (chkPot, fmm/driver.cc:157), so its printed error depends on what the heap
@@ -83,15 +86,21 @@ def test_dropin_matches_reference(oracle_mod, case):
         e_ref = rel_error(ref)
         out = {}
         for name, exe, extra in (("drop", DROPIN, {}), ("cli", CLI, {}),
-                                 ("mixed", DROPIN, {"KFMM_MIXED": "1"})):
+                                 ("mixed", DROPIN, {"KFMM_MIXED": "1"}),
+                                 ("hybrid", CLI, {"KFMM_CPU_SHARE_PPM": "1000000"})):
             path = os.path.join(td, name + ".bin")
             r = run(exe, [n, dist, ppb], KFMM_DUMP_POT=path, **extra, **env)
             assert r.returncode == 0, r.stderr[-500:]
             assert "== Timing for FMM3d ==" in r.stderr
             out[name] = (rel_error(r), np.fromfile(path, np.float64))
         assert "Code: b200-fp64" in run(DROPIN, [n, dist, ppb], **env).stdout
+        assert "Code: b200-fp64-hybrid" in run(CLI, [n, dist, ppb], KFMM_CPU_SHARE_PPM="1000000",
+                                               **env).stdout
     (e_drop, p_drop), (e_cli, p_cli), (e_mixed, p_mixed) = out["drop"], out["cli"], out["mixed"]
     d_drop, d_cli = _max_rel(p_drop, R["pot"]), _max_rel(p_cli, R["pot"])
+    # fmmd--b200 with the whole U list on the host (the fmmd--hybrid2 schedule)
+    d_hyb = _max_rel(out["hybrid"][1], R["pot"])
+    assert d_hyb <= max(1e-12, 5 * floor), d_hyb
     print(f"{case}: per-target vs reference: drop-in {d_drop:.2e} fmmd--b200 {d_cli:.2e} "
           f"(floor {floor:.2e}); printed error: reference {e_ref:.6e} drop-in {e_drop:.6e} "
           f"fmmd--b200 {e_cli:.6e} mixed {e_mixed:.6e}")
