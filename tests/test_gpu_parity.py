@@ -41,6 +41,7 @@ CASES = [
     ("uniform", 12000, 40, 5, 1),
     ("ellipseUniformAngles", 6000, 16, 8, 0),
     ("uniform", 65536, 128, 4, 1),  # the CPU-runnable benchmark configuration (fmmd--omp)
+    ("uniform", 8000, 24, 7, 0),
 ]
 # the metric's NP and leaf size (512 per box) at a size the reference runs in
 # seconds: depth 3-4 adaptive tree, V lists at depths 2-4, W and X lists
@@ -209,7 +210,13 @@ def test_adjacent_translation_spectra_ignored(K, cuda_ok, precision):
 
 
 MIXED_CASES = [("uniform", 65536, 128, 6, 0), ("uniform", 60000, 64, 4, 1),
-               ("ellipsoidSurface", 60000, 40, 4, 0), ("ellipseUniformAngles", 40000, 24, 5, 0)]
+               ("ellipsoidSurface", 60000, 40, 4, 0), ("ellipseUniformAngles", 40000, 24, 5, 0),
+               ("uniform", 40000, 32, 3, 0), ("uniform", 30000, 48, 7, 0),
+               ("uniform", 20000, 48, 8, 0)]
+# The mixed form's own rounding floor: FP32 pair terms, spectra and
+# Hadamard products leave ~1e-7 of the potentials; where the plain path's
+# error lies below that (NP >= 7) the mixed form's error is that floor.
+MIXED_FLOOR = 3e-7
 
 
 @pytest.mark.gpu
@@ -218,7 +225,9 @@ def test_mixed_precision_accuracy(K, oracle_mod, cuda_ok, case):
     """The mixed form (FP32 + compensated sums, FP64 final accumulation) is
     measured by the reference's own check, the relative L2 error against an
     exact FP64 direct sum on sampled targets: it must stay within 2x the
-    plain FP64 path's error; its distance to the plain path is reported."""
+    plain FP64 path's error, or within the mixed form's own rounding floor
+    (3e-7) where the plain error is smaller still (NP >= 7); its distance to
+    the plain path is reported."""
     dist, n, ppb, np_, coincide = case
     pts = K.generate_points(n, dist, coincide, 26, 400)
     tree = K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], ppb)
@@ -233,7 +242,7 @@ def test_mixed_precision_accuracy(K, oracle_mod, cuda_ok, case):
     print(f"{_ids(case)}: rel-L2 vs direct: plain {e_plain:.3e} mixed {e_mixed:.3e}; "
           f"mixed vs plain {vs_plain:.3e}")
     assert np.all(np.isfinite(mixed))
-    assert e_mixed <= 2.0 * e_plain
+    assert e_mixed <= max(2.0 * e_plain, MIXED_FLOOR)
 
 
 @pytest.mark.gpu
@@ -299,7 +308,8 @@ def test_mixed_downward_check_vs_plain(K, cuda_ok, case):
 
 
 TENSOR_CASES = [("uniform", 65536, 128, 6, 0, 2), ("uniform", 262144, 64, 4, 0, 2),
-                ("uniform", 300000, 32, 3, 1, 2), ("uniform", 150000, 16, 5, 0, 2)]
+                ("uniform", 300000, 32, 3, 1, 2), ("uniform", 150000, 16, 5, 0, 2),
+                ("uniform", 40000, 64, 8, 0, 2)]
 
 
 @pytest.mark.gpu
@@ -344,7 +354,7 @@ def test_tensor_core_hadamard(K, oracle_mod, cuda_ok, case):
     assert np.all(np.isfinite(tc))
     assert e_tc <= 2e-5
     assert vs_cuda <= 1e-6
-    assert e_tens <= 2.0 * e_plain
+    assert e_tens <= max(2.0 * e_plain, MIXED_FLOOR)
 
 
 @pytest.mark.gpu
