@@ -60,6 +60,18 @@ def test_tree_rejects_points_outside_root_box(K):
         K.Tree(pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"], 8)
 
 
+def test_tree_refuses_empty_point_sets(K):
+    """No sources, no targets or a leaf size below 1 is an argument error
+    (status KFMM_ERR_INVALID), not a tree: the evaluation needs both sets."""
+    pts = K.generate_points(50, "uniform")
+    z = np.zeros(0)
+    for args, ppb in (((z, z, z, z, z, z), 8), ((pts["sx"], pts["sy"], pts["sz"], z, z, z), 8),
+                      ((z, z, z, pts["tx"], pts["ty"], pts["tz"]), 8),
+                      ((pts["sx"], pts["sy"], pts["sz"], pts["tx"], pts["ty"], pts["tz"]), 0)):
+        with pytest.raises(K.KfmmError, match="bad argument"):
+            K.Tree(*args, ppb)
+
+
 def test_plan_create_argument_errors(K):
     L = K.lib()
     h = ctypes.c_void_p()
