@@ -448,12 +448,17 @@ inline long long key_of(int x, int y, int z) {
   return (long long)x | ((long long)y << 21) | ((long long)z << 42);
 }
 
+constexpr double kCostClassWidth = 1.05;  // cost ratio spanned by one job-order class
+
 // The near field's jobs: each target leaf's targets in chunks of 32 * rows
 // (rows: the tuning's job_rows, else 4 for mixed plans whose W-list surfaces
 // carry more than 1% of the pairs, else 6), ordered largest first by cost
-// class (target slots x sources, in classes 25% wide); within a class the
+// class (target slots x sources, in classes 5% wide); within a class the
 // jobs keep their tree order, so warps working at the same time read
-// neighbouring leaves' sources and the L2 cache serves the repeats.  The
+// neighbouring leaves' sources and the L2 cache serves the repeats (4M
+// points, NP=6 uniform / NP=4 ellipsoid surface, mixed near field: classes
+// 25% wide 4.44 / 2.32 ms, 12% 4.39 / 2.28, 5% 4.39 / 2.27, 100% 4.48 /
+// 2.50).  The
 // mixed near field runs with 5 resident blocks per SM on the same clouds
 // (or when the tuning says so).  Measured on 4M points on the ellipsoid
 // surface, NP=4, 256 per box: 2.32 ms against 2.50 ms with 6 blocks and 6
@@ -478,7 +483,7 @@ kfmm_status build_nf_jobs(kfmm_plan* p) {
   std::vector<std::pair<double, int>> key(jobs.size());
   for (size_t j = 0; j < jobs.size(); ++j) {
     const double cost = std::max(1.0, ns[j] * ((jobs[j].tcnt + 31) / 32));
-    key[j] = {-std::floor(std::log(cost) / std::log(1.25)), (int)j};
+    key[j] = {-std::floor(std::log(cost) / std::log(kCostClassWidth)), (int)j};
   }
   std::stable_sort(key.begin(), key.end(),
                    [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
@@ -744,7 +749,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     return kind == 0 ? d->src_num[node] : P;
   };
   // For the persistent P2P kernel: largest first, by cost class (target slots
-  // x sources, in classes 25% wide); within a class the jobs keep their tree
+  // x sources, in classes 5% wide); within a class the jobs keep their tree
   // order, so warps working at the same time read neighbouring leaves' sources
   // and the L2 cache serves the repeats.
   auto order_jobs = [&](std::vector<P2PJob>& jobs, const std::vector<int>& ent,
@@ -754,7 +759,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       double ns = 0;
       for (int k = jobs[j].ebeg; k < jobs[j].eend; ++k) ns += src_count(ent[k]);
       const double cost = std::max(1.0, ns * ((jobs[j].tcnt + 31) / 32));
-      key[j] = {-std::floor(std::log(cost) / std::log(1.25)), (int)j};
+      key[j] = {-std::floor(std::log(cost) / std::log(kCostClassWidth)), (int)j};
     }
     std::stable_sort(key.begin(), key.end(),
                      [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
