@@ -151,7 +151,9 @@ kfmm_status kfmm_plan_create_with_operators(const kfmm_tree_desc* tree, int np,
  *               reference's schedule), in FP64, while the GPU runs the rest;
  *               fixed at creation.  Such plans evaluate through
  *               kfmm_evaluate only (kfmm_run, kfmm_evaluate_async,
- *               kfmm_ulist_calc and batches refuse them). */
+ *               kfmm_ulist_calc and batches refuse them), and their
+ *               device-side potentials (kfmm_get_potentials_device,
+ *               kfmm_read_array) lack the host's share. */
 typedef struct {
   int nf_blocks;
   int job_rows;
