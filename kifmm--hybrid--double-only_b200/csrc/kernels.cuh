@@ -1,7 +1,8 @@
 // Device kernels of the KIFMM evaluator (sm_100a).  Included by plan.cu only.
 //
 // Data layout in HBM (all node-major, node = index into the BFS node array):
-//   src4[i]      leaf-ordered sources (x, y, z, w)            double4
+//   src4[i]      leaf-ordered sources (x, y, z, w), plain form double4
+//   src4f[i]     mixed form: (x, y, z) - leaf centre, w      float4
 //   trg4[i]      leaf-ordered targets (x, y, z, 0)            double4
 //   ctr[n]       node centre and radius (cx, cy, cz, r)       double4
 //   uden/dchk/dden[n*P + k]   upward equivalent density, downward check
@@ -1481,16 +1482,14 @@ __global__ void scatter_points_kernel(int n, const int* inv, const double* x, co
     out[inv[k]] = make_double4(x[k], y[k], z[k], w ? w[k] : 0.0);
 }
 
+// Mixed plans keep only the FP32 offsets (src4f); leaf[k]: source k's leaf.
 __global__ void scatter_sources_mixed_kernel(int n, const int* inv, const int* leaf,
                                              const double* x, const double* y, const double* z,
-                                             const double* w, const double4* ctr, double4* out,
-                                             float4* outf) {
+                                             const double* w, const double4* ctr, float4* outf) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int i = inv[k];
-    const double4 v = make_double4(x[k], y[k], z[k], w[k]);
-    const double4 c = ctr[leaf[i]];
-    out[i] = v;
-    outf[i] = make_float4((float)(v.x - c.x), (float)(v.y - c.y), (float)(v.z - c.z), (float)v.w);
+    const double4 c = ctr[leaf[k]];
+    outf[inv[k]] =
+        make_float4((float)(x[k] - c.x), (float)(y[k] - c.y), (float)(z[k] - c.z), (float)w[k]);
   }
 }
 

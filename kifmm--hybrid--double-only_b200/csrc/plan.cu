@@ -593,14 +593,6 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
       cf[i] = make_float4((float)ctr[i].x, (float)ctr[i].y, (float)ctr[i].z, (float)ctr[i].w);
     KF_TRY(upload(p, &p->ctrf, cf));
   }
-  if (p->prec == KFMM_MIXED) {
-    std::vector<int> leaf_of(d->num_src, 0);
-    for (int i = 0; i < nn; ++i)
-      if (d->child[i] == -1)
-        for (int k = 0; k < d->src_num[i]; ++k) leaf_of[d->src_beg[i] + k] = i;
-    KF_TRY(upload(p, &p->d_src_leaf, leaf_of));
-    KF_TRY(dalloc(p, &p->src4f, d->num_src));
-  }
   KF_TRY(upload(p, &p->d_depth, std::vector<int>(d->depth, d->depth + nn)));
   KF_TRY(upload(p, &p->d_src_beg, std::vector<int>(d->src_beg, d->src_beg + nn)));
   KF_TRY(upload(p, &p->d_src_num, std::vector<int>(d->src_num, d->src_num + nn)));
@@ -612,6 +604,16 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     for (int i = 0; i < d->num_trg; ++i) ti[d->trg_perm[i]] = i;
     KF_TRY(upload(p, &p->d_src_inv, si));
     KF_TRY(upload(p, &p->d_trg_inv, ti));
+    if (p->prec == KFMM_MIXED) {
+      // each source's leaf, by original index (the source gather reads it
+      // beside the coordinates, coalesced)
+      std::vector<int> leaf_of(d->num_src, 0);
+      for (int i = 0; i < nn; ++i)
+        if (d->child[i] == -1)
+          for (int k = 0; k < d->src_num[i]; ++k) leaf_of[d->src_perm[d->src_beg[i] + k]] = i;
+      KF_TRY(upload(p, &p->d_src_leaf, leaf_of));
+      KF_TRY(dalloc(p, &p->src4f, d->num_src));
+    }
   }
 
   // --- operators and surfaces
@@ -708,7 +710,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
   KF_TRY(dalloc(p, &p->o_tx, p->nt));
   KF_TRY(dalloc(p, &p->o_ty, p->nt));
   KF_TRY(dalloc(p, &p->o_tz, p->nt));
-  KF_TRY(dalloc(p, &p->src4, p->ns));
+  if (p->prec != KFMM_MIXED) KF_TRY(dalloc(p, &p->src4, p->ns));  // mixed kernels read src4f
   KF_TRY(dalloc(p, &p->trg4, p->nt));
   KF_TRY(dalloc(p, &p->pot_leaf, p->nt));
   KF_TRY(dalloc(p, &p->pot_orig, p->nt));
@@ -1398,7 +1400,7 @@ kfmm_status kfmm_set_sources_device(kfmm_plan* p, const double* sx, const double
   }
   if (p->prec == KFMM_MIXED) {
     scatter_sources_mixed_kernel<<<4 * p->num_sms, 256, 0, S(stream)>>>(
-        p->ns, p->d_src_inv, p->d_src_leaf, sx, sy, sz, den, p->ctr, p->src4, p->src4f);
+        p->ns, p->d_src_inv, p->d_src_leaf, sx, sy, sz, den, p->ctr, p->src4f);
   } else {
     scatter_points_kernel<<<4 * p->num_sms, 256, 0, S(stream)>>>(p->ns, p->d_src_inv, sx, sy, sz,
                                                                  den, p->src4);
