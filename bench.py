@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-solves sub-measurement")
     ap.add_argument("--batch", type=int, default=BATCH_SOLVES)
+    ap.add_argument("--no-sweep", action="store_true",
+                    help="skip the leaf-size sweep of the metric's workload")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="profile one form only (no JSON line)")
     ap.add_argument("--had-tensor", action="store_true",
@@ -239,10 +241,23 @@ def run_reference_cpu(n, max_steps, warmup, budget_s):
     pre, _ = _run_ref_once(exe, small, env)
     pre = min(pre, 0.5 * t)
     return {"value": n / (t - pre) / 1e6, "unit": "Mpts/s", "cores": cores, "kind": "reference",
+            "cpu_model": cpu_model(),
             "runs": len(times), "warmup_runs": done_warm, "seconds": times, "precompute_s": pre,
             "value_with_precompute": n / t / 1e6,
             "sample": f"fmmd--omp_sse_block {n} {DIST} {PPB} NP={NP}, {cores} threads; median "
                       f"Total Execution Time of {len(times)} runs - precompute"}
+
+
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or None."""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def reference_arm(args):
@@ -261,13 +276,55 @@ def reference_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_of(N_POINTS),
             "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample",
-                                                 "precompute_s", "value_with_precompute")},
+                                                 "precompute_s", "value_with_precompute",
+                                                 "cpu_model")},
             "e2e": {"value": v, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if res["runs"] < args.steps or res["warmup_runs"] < args.warmup:
         line["steps_note"] = (f"{res['warmup_runs']} warm-up and {res['runs']} timed runs of the "
                               f"{args.warmup} + {args.steps} requested fit the "
                               f"{REF_ARM_BUDGET_S:.0f} s budget of this arm")
     print(json.dumps(sig(line)))
+
+
+SWEEP_LEAF_SIZES = (32, 64, 128, 256, 512)
+
+
+def leaf_sweep(K, pts, sh, stream, steps, warmup, ids, direct):
+    """The metric's workload in the mixed form at each candidate leaf size:
+    device ms per kfmm_run (CUDA events on the launch stream, as `value`),
+    and the reference's check (rel-L2 against the direct sum at the same
+    sampled targets) at the fastest.  Trees are built on the device; each
+    plan is released before the next is made."""
+    import torch
+    ms_by, best = {}, None
+    args = [pts[k] for k in ("sx", "sy", "sz", "tx", "ty", "tz")]
+    for ppb in SWEEP_LEAF_SIZES:
+        tree = K.Tree(*args, ppb, device=True)
+        plan = K.Plan(tree, NP, K.MIXED)
+        try:
+            plan.set_points(pts, sh)
+            for _ in range(warmup):
+                plan.run(sh)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(steps):
+                plan.run(sh)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b) / steps
+            ms_by[str(ppb)] = ms
+            if best is None or ms < best[1]:
+                pot = plan.potentials(sh)[ids]
+                best = (ppb, ms, float(np.linalg.norm(pot - direct) / np.linalg.norm(direct)),
+                        tree.desc.num_nodes)
+        finally:
+            plan.close()
+            tree.close()
+    n = len(pts["sx"])
+    return sig({"ms_by_ppb": ms_by, "best_ppb": best[0], "best_ms": best[1],
+                "best_Mpts_s": n / best[1] / 1e3, "best_rel_l2_err": best[2],
+                "best_nodes": best[3]}, 4)
 
 
 def time_plan(K, plan, sh, stream, steps, warmup, barrier, world, dev):
@@ -388,6 +445,19 @@ def phase_rooflines(K, st, kern_mixed, pipes, hbm_gbs):
                        "unit": "GB/s HBM", "frac": b_had / (ms["hadamard"] * 1e-3) / hbm,
                        "fma_frac": had_flops / (ms["hadamard"] * 1e-3) / fma32}
     bound_s += max(b_had / hbm, had_flops / fma32)
+    # the V list as a whole (forward FFT, Hadamard, inverse FFT): compulsory
+    # bytes over its time against HBM, beside the reference's own per-pair
+    # byte model of the V list (fmm/driver.cc:120-136: per target box its
+    # FP64 effective values, per V pair a source spectrum and a translation
+    # vector, eff_data_size = (2np+2)(2np)^2 reals, fmm/trans.cc:107-115)
+    eff = (2 * NP + 2) * (2 * NP) ** 2
+    ref_bytes = 8.0 * eff * st["num_nodes"] + 16.0 * eff * st["v_pairs"]
+    v_ms = ms["fft_src"] + ms["hadamard"] + ms["ifft_trg"]
+    v_bytes = 2 * b_fft + b_had
+    out["vlist"] = {"ms": v_ms, "achieved": v_bytes / (v_ms * 1e-3) / 1e9, "peak": hbm_gbs,
+                    "unit": "GB/s HBM", "frac": v_bytes / (v_ms * 1e-3) / hbm,
+                    "compulsory_GB": v_bytes / 1e9, "ref_model_GB": ref_bytes / 1e9,
+                    "ref_model_rate_GBps": ref_bytes / (v_ms * 1e-3) / 1e9}
     total_ms = sum(ms.values())
     out["solve"] = {"roofline_ms": bound_s * 1e3, "measured_ms": total_ms,
                     "frac": bound_s * 1e3 / total_ms}
@@ -527,6 +597,13 @@ def main():
     e2e_ms = reduce_max(a.elapsed_time(b) / args.steps, world, dev)
     assert np.array_equal(hout.numpy(), pots["mixed"]), "e2e potentials differ from the resident run"
 
+    # ---- the same workload at the sweep-best leaf size (one GPU only: the
+    # replicas of a multi-GPU run report the metric's 512 alone)
+    sweep_res = None
+    if world == 1 and not args.no_sweep:
+        sweep_res = leaf_sweep(K, pts, sh, stream, max(1, min(args.steps, 5)),
+                               max(1, min(args.warmup, 2)), ids, direct)
+
     peaks = measured_peaks()
     hbm_gbs = peaks.get("hbm_gbs") or 6650.0
     pipes = K.measure_peaks()
@@ -556,7 +633,8 @@ def main():
             r = run_reference_cpu(n, 3, 0, CPU_BASELINE_BUDGET_S)
             if r:
                 cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample",
-                                         "precompute_s", "value_with_precompute", "runs")}
+                                         "precompute_s", "value_with_precompute", "runs",
+                                         "cpu_model")}
         except Exception as ex:  # reported, not fatal
             cpu = {"value": None, "error": str(ex)[:200]}
 
@@ -582,10 +660,13 @@ def main():
         "tree": {"nodes": st["num_nodes"], "u_pairs": pairs, "v_pairs": st["v_pairs"],
                  "build_s_host": tree_host_s, "build_s_device": tree_device_s},
         "batched": batched_res,
+        "leaf_sweep": sweep_res,
         "graph_4m": {"mixed_ms": graph_ms["mixed"], "fp64_ms": graph_ms["fp64"],
                      "mixed_over_fp64_direct": ms_fp64 / graph_ms["mixed"]},
         "phase_roofline": {k: ({"ms": v["ms"], "frac": v["frac"], "of": v["unit"].split()[-1]}
-                               if "ms" in v and k != "solve" else v) for k, v in phr.items()},
+                               if "ms" in v and k not in ("solve", "vlist") else
+                               {kk: vv for kk, vv in v.items() if kk not in ("peak", "unit")}
+                               if k == "vlist" else v) for k, v in phr.items()},
         "phases_ms": {"mixed": ph_mixed, "fp64": ph_fp64},
         "fp64": {"value": aggregate_mpts(n, world, ms_fp64), "ms_per_step": ms_fp64,
                  "rel_l2_err": err["fp64"], "near_field_frac": roof("fp64", nf_fp64)["frac"]},
