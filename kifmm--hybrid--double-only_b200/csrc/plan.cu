@@ -313,7 +313,10 @@ kfmm_status launch_gemms(const kfmm_plan* p, const std::vector<GemmBatch>& gs, c
     GemmArgs a{b.A, b.M, b.K, b.ksplit, b.nsplit > 1 ? p->splitk : nullptr, b.B, b.boff, b.C,
                b.coff, b.alpha, b.alpha_const, b.ncol, b.accumulate};
     dim3 grid(b.chunks, (b.ncol + kGemmBN - 1) / kGemmBN, b.nsplit);
-    gemm_fp64_dmma_kernel<<<grid, kGemmThreads, kGemmSmemBytes, st>>>(a, b.mrows);
+    if (b.accumulate)
+      gemm_fp64_dmma_kernel<true><<<grid, kGemmThreads, kGemmSmemBytes, st>>>(a, b.mrows);
+    else
+      gemm_fp64_dmma_kernel<false><<<grid, kGemmThreads, kGemmSmemBytes, st>>>(a, b.mrows);
     KF_CHECK_LAUNCH("gemm_fp64_dmma_kernel");
     if (b.nsplit > 1) {
       const size_t total = (size_t)b.ncol * b.M;
@@ -1196,8 +1199,10 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     KF_TRY(build_nf_jobs(p));
   }
 
-  KF_CUDA(cudaFuncSetAttribute(gemm_fp64_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kGemmSmemBytes));
+  KF_CUDA(cudaFuncSetAttribute(gemm_fp64_dmma_kernel<false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmemBytes));
+  KF_CUDA(cudaFuncSetAttribute(gemm_fp64_dmma_kernel<true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmemBytes));
   KF_CUDA(cudaFuncSetAttribute(hadamard_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kTcSmemBytes));
   KF_CUDA(cudaFuncSetAttribute(hadamard_fp32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
