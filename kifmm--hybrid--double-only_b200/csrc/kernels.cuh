@@ -897,89 +897,116 @@ __host__ __device__ constexpr int fft_boxes_per_block() {
 // (z, y) row, the y pass a (z, kx) column, the z pass a (ky, kx) column, and
 // each thread produces all outputs of its line from the <= np non-zero
 // inputs.
+// Five resident blocks per SM (shared memory allows five at NP = 6): with
+// the next group's values held in registers the unbounded kernel takes 168
+// registers and three blocks, measured slower on small and surface clouds.
 template <int NP, class C>
-__global__ void __launch_bounds__(kFFTThreads) fft_src_np_kernel(FFTParams p) {
+__global__ void __launch_bounds__(kFFTThreads, 5) fft_src_np_kernel(FFTParams p) {
   constexpr int N = 2 * NP, H = NP / 2, NK = NP + 1, B = fft_boxes_per_block<NP>();
   __shared__ double den[B][NP * NP * NP];
   __shared__ double2 X[B][NP * NP * NK];
   __shared__ double2 Y[B][NP * N * NK];
   __shared__ double cs[N], sn[N];
   constexpr int P = NP * NP * NP - (NP - 2) * (NP - 2) * (NP - 2);
+  constexpr int R = (B * P + kFFTThreads - 1) / kFFTThreads;  // surface values per thread
   __shared__ int node_s[B];
   __shared__ double scale_s[B];
   __shared__ int cell_s[P];  // surface point -> cell of the np^3 block
   const int tid = threadIdx.x;
-  const int b0 = blockIdx.x * B;
+  const int ngroups = (p.nboxes + B - 1) / B;
   if (tid < N) {
     cs[tid] = p.cs[tid];
     sn[tid] = p.sn[tid];
   }
-  if (tid < B) {
-    const int node = b0 + tid < p.nboxes ? p.nodes[b0 + tid] : -1;
-    node_s[tid] = node;
-    scale_s[tid] = node >= 0 ? ldexp(1.0, p.depth[node]) : 0.0;
-  }
   for (int q = tid; q < P; q += kFFTThreads)
     cell_s[q] = (p.surf_ijk[3 * q] * NP + p.surf_ijk[3 * q + 1]) * NP + p.surf_ijk[3 * q + 2];
-  for (int q = tid; q < B * NP * NP * NP; q += kFFTThreads) (&den[0][0])[q] = 0.0;
-  __syncthreads();
-  // the P surface values of each box: consecutive threads read consecutive
-  // values and scatter them into the box's np^3 block
-  for (int q = tid; q < B * P; q += kFFTThreads) {
-    const int bb = q / P, s = q % P;
-    const int node = node_s[bb];
-    if (node >= 0) den[bb][cell_s[s]] = p.pln[(size_t)node * p.P + s] * scale_s[bb];
-  }
-  __syncthreads();
-  // x: row (k = z, j = y), outputs kx
-  for (int q = tid; q < B * NP * NP; q += kFFTThreads) {
-    const int bb = q / (NP * NP), t = q % (NP * NP);
-    const int k = t / NP, j = t % NP;
-    double v[NP];
+  // Persistent: the block takes groups of B boxes in turn.  The P surface
+  // values of the next group (consecutive threads, consecutive values) and
+  // its nodes' scales are loaded into registers while this group is
+  // transformed, so the passes do not wait for global memory.
+  double pre[R];
+  int nx_node = -1;
+  double nx_scale = 0.0;
+  auto fetch = [&](int grp) {
 #pragma unroll
-    for (int i = 0; i < NP; ++i) v[i] = den[bb][(i * NP + j) * NP + k];
-#pragma unroll
-    for (int kx = 0; kx < NK; ++kx) {
-      double ar = 0, ai = 0;
-#pragma unroll
-      for (int i = 0; i < NP; ++i) {
-        const int m = (kx * (i + H)) % N;
-        ar = fma(v[i], cs[m], ar);
-        ai = fma(-v[i], sn[m], ai);
-      }
-      X[bb][(k * NP + j) * NK + kx] = make_double2(ar, ai);
+    for (int r = 0; r < R; ++r) {
+      const int q = tid + r * kFFTThreads, bb = q / P, s = q % P, b = grp * B + bb;
+      pre[r] = 0.0;
+      if (q < B * P && grp < ngroups && b < p.nboxes) pre[r] = p.pln[(size_t)p.nodes[b] * p.P + s];
     }
-  }
-  __syncthreads();
-  // y: column (k, kx), outputs ky
-  for (int q = tid; q < B * NP * NK; q += kFFTThreads) {
-    const int bb = q / (NP * NK), t = q % (NP * NK);
-    const int k = t / NK, kx = t % NK;
-    double2 v[NP], o[N];
+    if (tid < B) {
+      const int b = grp * B + tid;
+      nx_node = grp < ngroups && b < p.nboxes ? p.nodes[b] : -1;
+      nx_scale = nx_node >= 0 ? ldexp(1.0, p.depth[nx_node]) : 0.0;
+    }
+  };
+  fetch(blockIdx.x);
+  for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    __syncthreads();  // the previous group's passes are done with the shared arrays
+    if (tid < B) {
+      node_s[tid] = nx_node;
+      scale_s[tid] = nx_scale;
+    }
+    for (int q = tid; q < B * NP * NP * NP; q += kFFTThreads) (&den[0][0])[q] = 0.0;
+    __syncthreads();
+    // the group's surface values into the boxes' np^3 blocks
 #pragma unroll
-    for (int j = 0; j < NP; ++j) v[j] = X[bb][(k * NP + j) * NK + kx];
-    dft_fwd_pruned<NP>(v, o, cs, sn);
+    for (int r = 0; r < R; ++r) {
+      const int q = tid + r * kFFTThreads, bb = q / P, s = q % P;
+      if (q < B * P && node_s[bb] >= 0) den[bb][cell_s[s]] = pre[r] * scale_s[bb];
+    }
+    fetch(grp + gridDim.x);
+    __syncthreads();
+    // x: row (k = z, j = y), outputs kx
+    for (int q = tid; q < B * NP * NP; q += kFFTThreads) {
+      const int bb = q / (NP * NP), t = q % (NP * NP);
+      const int k = t / NP, j = t % NP;
+      double v[NP];
 #pragma unroll
-    for (int ky = 0; ky < N; ++ky) Y[bb][(k * N + ky) * NK + kx] = o[ky];
-  }
-  __syncthreads();
-  // z: column (ky, kx), outputs kz -> spectrum
-  C* out = (C*)p.specout;
-  for (int q = tid; q < B * N * NK; q += kFFTThreads) {
-    const int bb = q / (N * NK), t = q % (N * NK);
-    const int node = node_s[bb];
-    if (node < 0) continue;
-    const int ky = t / NK, kx = t % NK;
-    double2 v[NP], o[N];
+      for (int i = 0; i < NP; ++i) v[i] = den[bb][(i * NP + j) * NP + k];
 #pragma unroll
-    for (int k = 0; k < NP; ++k) v[k] = Y[bb][(k * N + ky) * NK + kx];
-    dft_fwd_pruned<NP>(v, o, cs, sn);
+      for (int kx = 0; kx < NK; ++kx) {
+        double ar = 0, ai = 0;
 #pragma unroll
-    for (int kz = 0; kz < N; ++kz) {
-      C e;
-      e.x = o[kz].x;
-      e.y = o[kz].y;
-      out[spec_index((kz * N + ky) * NK + kx, node, p.nn)] = e;
+        for (int i = 0; i < NP; ++i) {
+          const int m = (kx * (i + H)) % N;
+          ar = fma(v[i], cs[m], ar);
+          ai = fma(-v[i], sn[m], ai);
+        }
+        X[bb][(k * NP + j) * NK + kx] = make_double2(ar, ai);
+      }
+    }
+    __syncthreads();
+    // y: column (k, kx), outputs ky
+    for (int q = tid; q < B * NP * NK; q += kFFTThreads) {
+      const int bb = q / (NP * NK), t = q % (NP * NK);
+      const int k = t / NK, kx = t % NK;
+      double2 v[NP], o[N];
+#pragma unroll
+      for (int j = 0; j < NP; ++j) v[j] = X[bb][(k * NP + j) * NK + kx];
+      dft_fwd_pruned<NP>(v, o, cs, sn);
+#pragma unroll
+      for (int ky = 0; ky < N; ++ky) Y[bb][(k * N + ky) * NK + kx] = o[ky];
+    }
+    __syncthreads();
+    // z: column (ky, kx), outputs kz -> spectrum
+    C* out = (C*)p.specout;
+    for (int q = tid; q < B * N * NK; q += kFFTThreads) {
+      const int bb = q / (N * NK), t = q % (N * NK);
+      const int node = node_s[bb];
+      if (node < 0) continue;
+      const int ky = t / NK, kx = t % NK;
+      double2 v[NP], o[N];
+#pragma unroll
+      for (int k = 0; k < NP; ++k) v[k] = Y[bb][(k * N + ky) * NK + kx];
+      dft_fwd_pruned<NP>(v, o, cs, sn);
+#pragma unroll
+      for (int kz = 0; kz < N; ++kz) {
+        C e;
+        e.x = o[kz].x;
+        e.y = o[kz].y;
+        out[spec_index((kz * N + ky) * NK + kx, node, p.nn)] = e;
+      }
     }
   }
 }

@@ -171,6 +171,8 @@ struct kfmm_plan {
 
 namespace {
 
+int fft_src_resident(int np, bool mixed);  // resident blocks per SM of the forward FFT
+
 template <class T>
 kfmm_status dalloc(kfmm_plan* p, T** ptr, size_t count) {
   *ptr = nullptr;
@@ -1199,6 +1201,7 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
     KF_TRY(build_nf_jobs(p));
   }
 
+  fft_src_resident(p->np, p->prec == KFMM_MIXED);  // the occupancy query, before any capture
   KF_CUDA(cudaFuncSetAttribute(gemm_fp64_dmma_kernel<false>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmemBytes));
   KF_CUDA(cudaFuncSetAttribute(gemm_fp64_dmma_kernel<true>,
@@ -1245,29 +1248,62 @@ kfmm_status build_plan(kfmm_plan* p, const kfmm_tree_desc* d, const kfmm_operato
 
 inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
+// Resident blocks per SM of a kernel (queried once per instance).
+template <class Kern>
+int resident_blocks(Kern kern, int threads) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, 0) != cudaSuccess ||
+      occ < 1)
+    occ = 1;
+  return occ;
+}
+
+// Resident blocks per SM of the forward FFT kernel of NP; the first call (at
+// plan creation, outside any stream capture) makes the query.
 template <int NP>
-void fft_launch_np(bool mixed, bool forward, int nboxes, FFTParams f, cudaStream_t st) {
+int fft_src_resident(bool mixed) {
+  static const int occ32 = resident_blocks(fft_src_np_kernel<NP, float2>, kFFTThreads);
+  static const int occ64 = resident_blocks(fft_src_np_kernel<NP, double2>, kFFTThreads);
+  return mixed ? occ32 : occ64;
+}
+
+int fft_src_resident(int np, bool mixed) {
+  switch (np) {
+    case 3: return fft_src_resident<3>(mixed);
+    case 4: return fft_src_resident<4>(mixed);
+    case 5: return fft_src_resident<5>(mixed);
+    case 6: return fft_src_resident<6>(mixed);
+    case 7: return fft_src_resident<7>(mixed);
+    default: return fft_src_resident<8>(mixed);
+  }
+}
+
+template <int NP>
+void fft_launch_np(bool mixed, bool forward, int nboxes, int num_sms, FFTParams f,
+                   cudaStream_t st) {
   constexpr int B = fft_boxes_per_block<NP>();
   const int nblocks = (nboxes + B - 1) / B;
   f.nboxes = nboxes;
   if (forward) {
-    if (mixed) fft_src_np_kernel<NP, float2><<<nblocks, kFFTThreads, 0, st>>>(f);
-    else fft_src_np_kernel<NP, double2><<<nblocks, kFFTThreads, 0, st>>>(f);
+    // persistent: one wave of blocks, each taking groups of boxes in turn
+    const int grid = std::max(1, std::min(nblocks, num_sms * fft_src_resident<NP>(mixed)));
+    if (mixed) fft_src_np_kernel<NP, float2><<<grid, kFFTThreads, 0, st>>>(f);
+    else fft_src_np_kernel<NP, double2><<<grid, kFFTThreads, 0, st>>>(f);
   } else {
     if (mixed) ifft_trg_np_kernel<NP, float2><<<nblocks, kFFTThreads, 0, st>>>(f);
     else ifft_trg_np_kernel<NP, double2><<<nblocks, kFFTThreads, 0, st>>>(f);
   }
 }
 
-kfmm_status launch_fft(int np, bool mixed, bool forward, int nboxes, const FFTParams& f,
-                       void* stream) {
+kfmm_status launch_fft(int np, bool mixed, bool forward, int nboxes, int num_sms,
+                       const FFTParams& f, void* stream) {
   switch (np) {
-    case 3: fft_launch_np<3>(mixed, forward, nboxes, f, S(stream)); break;
-    case 4: fft_launch_np<4>(mixed, forward, nboxes, f, S(stream)); break;
-    case 5: fft_launch_np<5>(mixed, forward, nboxes, f, S(stream)); break;
-    case 6: fft_launch_np<6>(mixed, forward, nboxes, f, S(stream)); break;
-    case 7: fft_launch_np<7>(mixed, forward, nboxes, f, S(stream)); break;
-    case 8: fft_launch_np<8>(mixed, forward, nboxes, f, S(stream)); break;
+    case 3: fft_launch_np<3>(mixed, forward, nboxes, num_sms, f, S(stream)); break;
+    case 4: fft_launch_np<4>(mixed, forward, nboxes, num_sms, f, S(stream)); break;
+    case 5: fft_launch_np<5>(mixed, forward, nboxes, num_sms, f, S(stream)); break;
+    case 6: fft_launch_np<6>(mixed, forward, nboxes, num_sms, f, S(stream)); break;
+    case 7: fft_launch_np<7>(mixed, forward, nboxes, num_sms, f, S(stream)); break;
+    case 8: fft_launch_np<8>(mixed, forward, nboxes, num_sms, f, S(stream)); break;
     default: set_error("launch_fft: NP out of range"); return KFMM_ERR_UNSUPPORTED;
   }
   KF_CHECK_LAUNCH(forward ? "fft_src_np_kernel" : "ifft_trg_np_kernel");
@@ -1480,7 +1516,7 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
     f.nodes = p->fft_nodes;
     f.pln = p->uden;
     f.specout = p->spec;
-    KF_TRY(launch_fft(p->np, mixed, true, p->n_fft, f, stream));
+    KF_TRY(launch_fft(p->np, mixed, true, p->n_fft, p->num_sms, f, stream));
   }
   mark(p, 3, S(stream));
   if (p->n_groups) {
@@ -1528,7 +1564,7 @@ kfmm_status kfmm_vlist_calc(kfmm_plan* p, void* stream) {
     f.nodes = p->ifft_nodes;
     f.specin = p->effv;
     f.plnout = p->dchk;
-    KF_TRY(launch_fft(p->np, mixed, false, p->n_ifft, f, stream));
+    KF_TRY(launch_fft(p->np, mixed, false, p->n_ifft, p->num_sms, f, stream));
   }
   return KFMM_OK;
 }
