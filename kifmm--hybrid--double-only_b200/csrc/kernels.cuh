@@ -1405,8 +1405,10 @@ __global__ void __launch_bounds__(kHad32Threads, 1) hadamard_fp32_kernel(Had32Pa
 // Rows whose 8 entries are all absent (windows at the domain's faces, and
 // the many empty boxes around clouds on surfaces) are not visited: the plan
 // gives each window a mask of its rows that hold an entry (4M points on the
-// ellipsoid surface: 1.19 -> 0.65 ms; uniform cube: -2%).  The zero
-// translation values of adjacent offsets are multiplied like the others:
+// ellipsoid surface: 1.19 -> 0.65 ms; uniform cube: -2%).  The four centre
+// rows, where every member pair meets the zero translation values of the
+// adjacent offsets, run as separate runs of a body that skips them (1.527
+// -> 1.510 ms at 4M, NP=6); elsewhere they are multiplied like the others:
 // row bodies specialised on which member pairs meet an adjacent row (ten
 // variants, dispatched per row) were measured 14% slower on the uniform cube.
 constexpr int kHadPairThreads = 384;
@@ -1457,6 +1459,39 @@ __device__ __forceinline__ void had_pair_row(unsigned long long (&A)[16],
   }
 }
 
+// A centre row of the window (wy and wz in {2, 3}): every member pair (cy, cz)
+// meets it at |dy|, |dz| <= 1, so its translation values k = 2..4 (dx = -1,
+// 0, 1: adjacent offsets, zero spectra) are neither loaded nor multiplied.
+__device__ __forceinline__ void had_pair_row_centre(unsigned long long (&A)[16],
+                                                    unsigned long long (&B)[16],
+                                                    const unsigned long long (&sr)[8],
+                                                    const unsigned long long (&si)[8],
+                                                    const unsigned long long* trow0) {
+#pragma unroll
+  for (int cyz = 0; cyz < 4; ++cyz) {
+    const int cy = cyz >> 1, cz = cyz & 1;
+    const unsigned long long* trow = trow0 - (cz * 49 + cy * 7) * kFB;
+    unsigned long long t[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+      if (k < 2 || k > 4) t[k] = trow[k * kFB];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int wx = 0; wx < 6; ++wx)
+#pragma unroll
+        for (int cx = 0; cx < 2; ++cx) {
+          const int k = wx - cx + 1;
+          if (k >= 2 && k <= 4) continue;
+          const int c = h * 8 + cx * 4 + cy * 2 + cz;
+          asm("fma.rn.f32x2 %0, %2, %3, %0;\n"
+              "fma.rn.f32x2 %1, %2, %4, %1;\n"
+              : "+l"(A[c]), "+l"(B[c])
+              : "l"(t[k]), "l"(sr[wx + 2 * h]), "l"(si[wx + 2 * h]));
+        }
+  }
+}
+
 __global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(HadPairParams p) {
   extern __shared__ __align__(128) unsigned char had32_dyn[];
   __shared__ int win[kHadPairWarps][288];
@@ -1480,9 +1515,8 @@ __global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(
     unsigned long long A[16], B[16];
 #pragma unroll
     for (int c = 0; c < 16; ++c) A[c] = B[c] = 0ull;
-    // the first half-window's sums go to shared memory (FP64) before the
-    // first row of z-planes 3-5, or at the end if there is none
-    bool flushed = false;
+    // the first half-window's sums go to shared memory (FP64) once its rows
+    // are done
     auto flush = [&]() {
 #pragma unroll
       for (int c = 0; c < 16; ++c) {
@@ -1490,39 +1524,53 @@ __global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(
         sums[(2 * c + 1) * 32] = (double)hi_of(A[c]) + (double)lo_of(B[c]);
         A[c] = B[c] = 0ull;
       }
-      flushed = true;
     };
-    int row = rows ? __ffsll((long long)rows) - 1 : 36;
-    unsigned long long nxt[8];
-    if (row < 36) {
-#pragma unroll
-      for (int x = 0; x < 8; ++x) {
-        const int sid = w[row * 8 + x];
-        nxt[x] = sid >= 0 ? spec[(size_t)sid * kFB] : 0ull;
-      }
-    }
-    while (row < 36) {
-      rows &= rows - 1;
-      const int next = rows ? __ffsll((long long)rows) - 1 : 36;
-      unsigned long long sr[8], si[8];  // {sr, sr}, {si, si}
-#pragma unroll
-      for (int x = 0; x < 8; ++x) {
-        sr[x] = pack2(lo_of(nxt[x]), lo_of(nxt[x]));
-        si[x] = pack2(hi_of(nxt[x]), hi_of(nxt[x]));
-      }
-      if (next < 36) {
+    // Rows in four runs: the first half-window's other rows, its centre rows
+    // (14, 15), the flush, the second half's centre rows (20, 21), then its
+    // other rows; the centre rows skip the zero adjacent offsets.
+    constexpr unsigned long long kLow = (1ull << 18) - 1;  // z-planes 0-2
+    constexpr unsigned long long kCentre = (1ull << 14) | (1ull << 15) | (1ull << 20) | (1ull << 21);
+#pragma unroll 1
+    for (int run = 0; run < 4; ++run) {
+      if (run == 2) flush();
+      unsigned long long m =
+          rows & (run < 2 ? kLow : ~kLow) & (run == 1 || run == 2 ? kCentre : ~kCentre);
+      int row = m ? __ffsll((long long)m) - 1 : 36;
+      unsigned long long nxt[8];
+      if (row < 36) {
 #pragma unroll
         for (int x = 0; x < 8; ++x) {
-          const int sid = w[next * 8 + x];
+          const int sid = w[row * 8 + x];
           nxt[x] = sid >= 0 ? spec[(size_t)sid * kFB] : 0ull;
         }
       }
-      const int wy = row % 6, wz = row / 6;
-      if (!flushed && wz >= 3) flush();
-      had_pair_row(A, B, sr, si, tsm + ((wz + 1) * 49 + (wy + 1) * 7) * kFB + f);
-      row = next;
+      auto walk = [&](auto centre) {
+        while (row < 36) {
+          m &= m - 1;
+          const int next = m ? __ffsll((long long)m) - 1 : 36;
+          unsigned long long sr[8], si[8];  // {sr, sr}, {si, si}
+#pragma unroll
+          for (int x = 0; x < 8; ++x) {
+            sr[x] = pack2(lo_of(nxt[x]), lo_of(nxt[x]));
+            si[x] = pack2(hi_of(nxt[x]), hi_of(nxt[x]));
+          }
+          if (next < 36) {
+#pragma unroll
+            for (int x = 0; x < 8; ++x) {
+              const int sid = w[next * 8 + x];
+              nxt[x] = sid >= 0 ? spec[(size_t)sid * kFB] : 0ull;
+            }
+          }
+          const int wy = row % 6, wz = row / 6;
+          const unsigned long long* trow0 = tsm + ((wz + 1) * 49 + (wy + 1) * 7) * kFB + f;
+          if constexpr (decltype(centre)::value) had_pair_row_centre(A, B, sr, si, trow0);
+          else had_pair_row(A, B, sr, si, trow0);
+          row = next;
+        }
+      };
+      if (run == 1 || run == 2) walk(std::true_type{});
+      else walk(std::false_type{});
     }
-    if (!flushed) flush();
 #pragma unroll
     for (int c = 0; c < 16; ++c) {
       const int m = mem[slot][c];
