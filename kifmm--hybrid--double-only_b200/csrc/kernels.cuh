@@ -1530,37 +1530,47 @@ __global__ void __launch_bounds__(kHadPairThreads, 1) hadamard_fp32_pair_kernel(
     // other rows; the centre rows skip the zero adjacent offsets.
     constexpr unsigned long long kLow = (1ull << 18) - 1;  // z-planes 0-2
     constexpr unsigned long long kCentre = (1ull << 14) | (1ull << 15) | (1ull << 20) | (1ull << 21);
+    auto run_rows = [&](int run) {
+      return rows & (run < 2 ? kLow : ~kLow) & (run == 1 || run == 2 ? kCentre : ~kCentre);
+    };
+    auto first_after = [&](int run) {  // first row of the runs after `run`, 36 if none
+      for (int q = run + 1; q < 4; ++q) {
+        const unsigned long long mm = run_rows(q);
+        if (mm) return __ffsll((long long)mm) - 1;
+      }
+      return 36;
+    };
+    // the next row's source spectra are loaded while the current row is
+    // multiplied, across the runs' boundaries too
+    unsigned long long nxt[8];
+    auto fetch = [&](int r) {
+#pragma unroll
+      for (int x = 0; x < 8; ++x) {
+        const int sid = w[r * 8 + x];
+        nxt[x] = sid >= 0 ? spec[(size_t)sid * kFB] : 0ull;
+      }
+    };
+    {
+      const int r0 = first_after(-1);
+      if (r0 < 36) fetch(r0);
+    }
 #pragma unroll 1
     for (int run = 0; run < 4; ++run) {
       if (run == 2) flush();
-      unsigned long long m =
-          rows & (run < 2 ? kLow : ~kLow) & (run == 1 || run == 2 ? kCentre : ~kCentre);
+      unsigned long long m = run_rows(run);
       int row = m ? __ffsll((long long)m) - 1 : 36;
-      unsigned long long nxt[8];
-      if (row < 36) {
-#pragma unroll
-        for (int x = 0; x < 8; ++x) {
-          const int sid = w[row * 8 + x];
-          nxt[x] = sid >= 0 ? spec[(size_t)sid * kFB] : 0ull;
-        }
-      }
       auto walk = [&](auto centre) {
         while (row < 36) {
           m &= m - 1;
           const int next = m ? __ffsll((long long)m) - 1 : 36;
+          const int ahead = next < 36 ? next : first_after(run);
           unsigned long long sr[8], si[8];  // {sr, sr}, {si, si}
 #pragma unroll
           for (int x = 0; x < 8; ++x) {
             sr[x] = pack2(lo_of(nxt[x]), lo_of(nxt[x]));
             si[x] = pack2(hi_of(nxt[x]), hi_of(nxt[x]));
           }
-          if (next < 36) {
-#pragma unroll
-            for (int x = 0; x < 8; ++x) {
-              const int sid = w[next * 8 + x];
-              nxt[x] = sid >= 0 ? spec[(size_t)sid * kFB] : 0ull;
-            }
-          }
+          if (ahead < 36) fetch(ahead);
           const int wy = row % 6, wz = row / 6;
           const unsigned long long* trow0 = tsm + ((wz + 1) * 49 + (wy + 1) * 7) * kFB + f;
           if constexpr (decltype(centre)::value) had_pair_row_centre(A, B, sr, si, trow0);
